@@ -1,0 +1,345 @@
+"""Throughput benchmark of the IF-RK4 pseudo-spectral step (w, r1, r2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl qaf|reference] [--dtype f32|f64]
+
+Workload: the "plain throughput" configuration — 1024 x 1024 periodic grid,
+L = 16 pi, friction solver parameters Re = 1 (nu = 1), Rf = 0.1 (mu = 0.1),
+Er = 1, lambda = 0.1, activity Ra = 1, IF-RK4 with dt = 5e-4, seeded random Q
+~ U(-0.01, 0.01) (seed 1), w = 0; FP32 by default (--dtype f64 for FP64).
+A bench step is one solver time step; the metric is grid-point steps per
+second of the whole job.
+
+Arms:
+  qaf (default)   this library. `value`: the device-resident state advanced one
+                  step at a time with CUDA events around each step and the L2
+                  flushed (a 256 MiB write) between timed steps. `e2e`: the same
+                  through the public API with host I/O every step — the activity
+                  field uploaded from pinned memory (the control input of a
+                  closed-loop run) and the step's energy/enstrophy read back.
+  reference       the reference's own CUDA build (oracle/_ref, built from its
+                  unmodified headers; FP32 through the macro shim, FP64 as
+                  shipped) timed on the same GPU with CUDA events. The reference
+                  has no CPU implementation of the path.
+
+Multi-GPU: the path does not shard (one grid per GPU); N GPUs run N
+independent replicas under torchrun, value = total over ranks / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "nature-control_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "grid-pt*steps/s at 1024^2, IF-RK4 (w, r1, r2)"
+UNIT = "grid-pt*steps/s"
+N_GRID = 1024
+L = 16 * 3.141592653589793
+DT = 5e-4
+SEED = 1
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["qaf", "reference"], default="qaf")
+    ap.add_argument("--dtype", choices=["f32", "f64"], default="f32")
+    ap.add_argument("--n", type=int, default=N_GRID)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a timed region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap,utilization.gpu"
+
+    def __init__(self, local_rank):
+        import torch
+        self.uuid = None
+        try:
+            self.uuid = str(torch.cuda.get_device_properties(local_rank).uuid)
+            if not self.uuid.startswith("GPU-"):
+                self.uuid = "GPU-" + self.uuid
+        except Exception:
+            pass
+        self.proc = None
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd.insert(1, f"--id={self.uuid}")
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[2:7], float(parts[7]) if parts[7] not in ("[N/A]", "") else 0.0))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        loaded = [r for r in rows if r[3] > 0] or rows
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in loaded:
+            for nm, v in zip(names[1:], r[2][1:]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(loaded)}
+
+
+def initial_state(mesh, seed):
+    """Seeded random-Q state (include/qaf_init.h), transformed by the library."""
+    import numpy as np
+    import torch
+
+    import oracle as O   # only for the numpy restatement of the seeded generator
+    w, r1, r2 = O.random_q_init(seed, mesh.nx)
+    return [mesh.fwd_trans(torch.from_numpy(a).to("cuda", dtype=mesh.real_dtype)) for a in (w, r1, r2)]
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def cpu_baseline(n, steps, dtype_name):
+    """The FP64 host oracle (a restatement of the reference's scheme) on the
+    host cores, on a bounded sample of the same workload."""
+    import oracle as O
+    p = O.params(n=n, L=L, dt=DT)
+    s0 = O.initial_spectra(SEED, n)
+    O.step(p, *s0, 1)          # warm the FFT plans
+    t0 = time.perf_counter()
+    O.step(p, *s0, steps)
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("QAF_ORACLE_THREADS", os.cpu_count() or 1))
+    return {"value": n * n * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} IF-RK4 steps of the {n}^2 workload in FP64 ({dt:.1f} s) with the host oracle, "
+                      f"which follows the reference's operation sequence (~120 2D FFTs per step)"}
+
+
+def run_qaf(a, world, rank, local):
+    import numpy as np
+    import torch
+
+    import qaf
+
+    dtype = qaf.F32 if a.dtype == "f32" else qaf.F64
+    n = a.n
+    mesh = qaf.Mesh(n, lx=L, dtype=dtype)
+    p = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=DT, q_lin=1.0, advect_omega=1)
+    state = initial_state(mesh, SEED)
+    mesh.load(*state)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+
+    # ---- device-resident throughput -------------------------------------
+    for _ in range(a.warmup):
+        mesh.advance(p, 1)
+    barrier(world)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    l0 = mesh.launch_count()
+    with ClockSampler(local) as clk:
+        barrier(world)
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record()
+            mesh.advance(p, 1)
+            e1.record()
+        barrier(world)
+    launches = mesh.launch_count() - l0
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    ms = max_over_ranks(ms, world)
+    mesh.check_finite()
+    value = world * n * n * a.steps / (ms * 1e-3)
+
+    # ---- per-kernel timing for the roofline (CUDA events on the launching stream)
+    row_ms, col_ms, _ = mesh.advance_timed(p, max(4, min(a.steps, 50)))
+    real_b = 4 if dtype == qaf.F32 else 8
+    ca = (n // 2 + 1) * n * 2 * real_b                 # one complex spectral array
+    # algorithmic bytes per launch (three-pass model): row pass reads 9 and writes 11
+    # arrays; the column pass (combine + stage update + next stage's inverse) moves 35
+    kern = {"row": (row_ms, 20 * ca), "column": (col_ms, 35 * ca)}
+    dom = max(kern, key=lambda k: kern[k][0])
+    k_ms, k_bytes = kern[dom]
+    peak, peak_kind = peaks()
+    achieved = k_bytes / (k_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"{dom}_{a.dtype}_{n}")
+        except Exception:
+            traffic = None
+
+    # ---- end to end through the public API, host I/O every step ----------
+    import oracle as O
+    x = np.arange(n) * L / n
+    alpha_host = torch.ones((n, n), dtype=mesh.real_dtype).pin_memory()
+    alpha_dev = torch.empty((n, n), dtype=mesh.real_dtype, device="cuda")
+    pe = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=DT, alpha_field=alpha_dev)
+    for _ in range(2):
+        alpha_dev.copy_(alpha_host, non_blocking=True)
+        mesh.advance(pe, 1)
+        mesh.last_diagnostics()
+    barrier(world)
+    e2e_steps = max(10, a.steps // 2)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(e2e_steps)]
+    diags = []
+    for e0, e1 in ev2:
+        flush.zero_()
+        e0.record()
+        alpha_dev.copy_(alpha_host, non_blocking=True)      # H2D: the step's activity field
+        mesh.advance(pe, 1)
+        diags.append(mesh.last_diagnostics())               # D2H: the step's energy, enstrophy
+        e1.record()
+    barrier(world)
+    ms2 = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in ev2), world)
+    e2e = {"value": world * n * n * e2e_steps / (ms2 * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": n * n * real_b, "d2h_bytes_per_step": 2 * 8 + 4}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": a.dtype, "data": "synthetic (seeded random Q ~ U(-0.01,0.01), w = 0)",
+        "config": {"workload": f"plain throughput {n}x{n}, L=16pi, IF-RK4 dt={DT}, Re=1 Rf=0.1 Er=1 lambda=0.1 Ra=1",
+                   "grid": n, "integrator": "IF-RK4", "dt": DT, "seed": SEED, "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MiB write) between timed steps"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": k_bytes, "ms_per_launch": k_ms,
+                     "row_ms": row_ms, "col_ms": col_ms},
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(n, a.cpu_sample_steps, a.dtype)
+    return line
+
+
+def run_reference(a, world, rank, local):
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness_f32" if a.dtype == "f32" else "ref_harness")
+    if not os.path.exists(exe):
+        return {"impl": "reference", "unavailable": "the reference's CUDA build (oracle/_ref) was not built: "
+                                                    "its sources were not present when build() ran"}
+    cmd = [exe, "time", "--n", str(a.n), "--L", repr(L), "--dt", repr(DT), "--seed", str(SEED),
+           "--re", "1", "--er", "1", "--rf", "0.1", "--lambda", "0.1", "--alpha", "1",
+           "--warmup", str(a.warmup), "--timed", str(a.steps)]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
+    with ClockSampler(local) as clk:
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        return {"impl": "reference", "unavailable": f"reference build exited {r.returncode}: {r.stderr.strip()[-200:]}"}
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    ms = out["ms_per_step"]
+    value = a.n * a.n / (ms * 1e-3)
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": a.dtype, "data": "synthetic (seeded random Q ~ U(-0.01,0.01), w = 0)",
+        "config": {"workload": f"plain throughput {a.n}x{a.n}, L=16pi, IF-RK4 dt={DT}, Re=1 Rf=0.1 Er=1 lambda=0.1 Ra=1",
+                   "grid": a.n, "integrator": "IF-RK4", "dt": DT, "seed": SEED, "parallelism": "single GPU",
+                   "l2": "working set (22 fields, ~185 MB in FP32) larger than L2"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"{a.steps} steps of the reference's own CUDA build (friction.cu step sequence, "
+                                   f"unmodified headers{', FP32 macro shim' if a.dtype == 'f32' else ''}) on the B200; "
+                                   "the reference has no CPU implementation of the path"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    }
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        # one rank runs the reference; under torchrun the others exit without work
+        rank, local = int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+        if rank == 0:
+            print(json.dumps(run_reference(a, 1, rank, local)), flush=True)
+        return
+    world, rank, local = dist_init()
+    import torch
+    torch.cuda.set_device(local)
+    line = run_qaf(a, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,173 @@
+/*
+ * qaf.h — C ABI of the B200 pseudo-spectral active-nematic solver.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, no C++ or torch types.
+ * Every call returns a qaf_status. Device pointers are CUDA device pointers;
+ * `stream` is a cudaStream_t passed as void* (NULL = the legacy default
+ * stream, like the reference, which runs everything on it).
+ *
+ * Precision is a property of the mesh (QAF_F64 = the reference's Qreal =
+ * double, QAF_F32 = float); every real/complex pointer passed with a mesh
+ * points to that mesh's type (complex = interleaved re, im).
+ *
+ * Layouts are the reference's (Basic/Mesh.cuh:48-129):
+ *   physical field  nx*ny reals, index i + j*nx
+ *   spectrum        (nx/2+1)*ny complex, index i + j*(nx/2+1)
+ *
+ * Each entry point below names the reference interface it replaces
+ * (file:line in whpy/nature-control).
+ *
+ * Scratch: a mesh owns its scratch buffers (as the reference's Mesh owns
+ * mesh->spec / mesh->phys, Mesh.cuh:66-77), so calls on one mesh must not
+ * overlap in time (the same restriction as the reference's FwdTrans/BwdTrans).
+ * Different meshes are independent.
+ */
+#ifndef QAF_H
+#define QAF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    QAF_OK = 0,
+    QAF_ERR_INVALID = 1,      /* bad argument (null handle/pointer, bad size, bad enum) */
+    QAF_ERR_UNSUPPORTED = 2,  /* valid but not built (e.g. a grid size without kernels) */
+    QAF_ERR_CUDA = 3,         /* a CUDA runtime call failed; see qaf_last_error() */
+    QAF_ERR_NONFINITE = 4,    /* the state holds Inf/NaN (qaf_check_finite) */
+    QAF_ERR_ALLOC = 5         /* device allocation failed */
+} qaf_status;
+
+typedef enum { QAF_F32 = 0, QAF_F64 = 1 } qaf_dtype;
+
+/* Integrators: IF-Euler (TimeIntegration/IFE.cuh:15-25), IF-RK2
+ * (TimeIntegration/IFRK2.cuh:16-51) and IF-RK4 (TimeIntegration/RK4.cuh:12-74). */
+typedef enum { QAF_IFE = 0, QAF_IFRK2 = 1, QAF_IFRK4 = 2 } qaf_integrator;
+
+typedef struct {
+    int nx, ny;        /* grid points (nx even); the fused stepper needs nx == ny */
+    double lx, ly;     /* domain lengths */
+    qaf_dtype dtype;
+} qaf_mesh_desc;
+
+/* Physical parameters of InertialFriction/friction/Qsolver.cuh and friction.cu:100-105. */
+typedef struct {
+    double re;          /* Re: w viscosity 1/Re, L_w = (-k^2 - Rf)/Re (wlin_func :20-30) */
+    double er;          /* Er: active/elastic stress scale 1/(Er Re) (PiDeriv :154-164) */
+    double rf;          /* Rf: friction */
+    double lambda;      /* flow-alignment parameter */
+    double alpha;       /* constant activity Ra, used when alpha_field is NULL */
+    const void* alpha_field;  /* optional physical activity field Ra(x), nx*ny reals on the device */
+    double dt;
+    double q_lin;       /* L_Q = -k^2 + q_lin (hard-wired 1.0 in r1lin_func/r2lin_func :32-54) */
+    int advect_omega;   /* 1: keep -div(u w) in N_w (friction variant); 0: drop it (beginning2) */
+} qaf_params;
+
+typedef struct qaf_mesh qaf_mesh;
+
+/* ---- library ---------------------------------------------------------- */
+const char* qaf_version(void);
+/* message of the last failing call on this host thread ("" if none) */
+const char* qaf_last_error(void);
+/* 1 if the fused stepper has kernels for an n x n grid of this dtype */
+int qaf_supported(int n, qaf_dtype dtype);
+
+/* ---- mesh (Basic/Mesh.cuh:48-113; Field :115-129) ---------------------- */
+qaf_status qaf_mesh_create(const qaf_mesh_desc* desc, qaf_mesh** out);
+qaf_status qaf_mesh_destroy(qaf_mesh* mesh);
+/* sizes in bytes of one physical field and one spectrum (physsize/specsize, Mesh.cuh:73-75) */
+qaf_status qaf_mesh_sizes(const qaf_mesh* mesh, size_t* phys_bytes, size_t* spec_bytes);
+/* device allocation of one field pair, like new Field(mesh) (Mesh.cuh:115-129) */
+qaf_status qaf_field_alloc(const qaf_mesh* mesh, void** phys, void** spec);
+qaf_status qaf_field_free(void* phys, void* spec);
+/* kx, ky, k^2 and the 2/3 mask tables, (nx/2+1)*ny reals each, host memory
+ * (waveinit / cutoff_func, Mesh.cuh:6-46); any pointer may be NULL */
+qaf_status qaf_mesh_tables(const qaf_mesh* mesh, void* kx, void* ky, void* k2, void* cutoff);
+
+/* ---- transforms (FldOp/QFldfuncs.cuh:45-55) ----------------------------- */
+/* FwdTrans: unnormalised R2C, phys -> spec */
+qaf_status qaf_fwd_trans(qaf_mesh* mesh, const void* phys, void* spec, void* stream);
+/* BwdTrans: C2R with the 1/(nx ny) scaling, spec -> phys. The input is not
+ * modified; its kx = 0 and kx = nx/2 columns contribute their Hermitian parts
+ * (what the reference's cuFFT C2R does). */
+qaf_status qaf_bwd_trans(qaf_mesh* mesh, const void* spec, void* phys, void* stream);
+/* symmetry_func (QFldfuncs.cuh:18-44): the in-place kx = 0 symmetrisation that
+ * the reference's BwdTrans applies to its input, for callers that rely on it */
+qaf_status qaf_symmetrize(qaf_mesh* mesh, void* spec, void* stream);
+
+/* ---- spectral operators (QFldfuncs.cuh:165-224) ------------------------- */
+qaf_status qaf_xderiv(qaf_mesh* mesh, const void* in, void* out, void* stream);     /* xDeriv */
+qaf_status qaf_yderiv(qaf_mesh* mesh, const void* in, void* out, void* stream);     /* yDeriv */
+qaf_status qaf_laplacian(qaf_mesh* mesh, const void* in, void* out, void* stream);  /* Laplacian */
+qaf_status qaf_vel(qaf_mesh* mesh, const void* w, void* u, void* v, void* stream);  /* vel_func */
+/* dealias (Qsolver.cuh:314-322): spec *= 2/3 mask, in place */
+qaf_status qaf_dealias(qaf_mesh* mesh, void* spec, void* stream);
+
+/* ---- IF tables and stage kernels ---------------------------------------- */
+/* wlin_func (which = 0) / r1lin_func, r2lin_func (which = 1), Qsolver.cuh:20-54:
+ * IF = exp(L dt), IFh = exp(L dt / 2), (nx/2+1)*ny reals each, device memory */
+qaf_status qaf_if_tables(qaf_mesh* mesh, const qaf_params* p, int which, void* IF, void* IFh, void* stream);
+/* integrate_func0D..4D of RK4.cuh:12-74 (integrator QAF_IFRK4, stage 0..4),
+ * IF::IFRK2::integrate_func0D..2D (QAF_IFRK2, stage 0..2) and
+ * IF::IFE::integrate_func1D (QAF_IFE, stage 1; curr unused) on reference-layout
+ * spectra; `nonl` is unused at stage 0 */
+qaf_status qaf_integrate(qaf_mesh* mesh, qaf_integrator integ, int stage, const void* old_spec, void* curr_spec,
+                         void* new_spec, const void* nonl_spec, const void* IF, const void* IFh, double dt,
+                         void* stream);
+
+/* ---- the hot path -------------------------------------------------------- */
+/* Nonlinear right-hand sides N_w, N_r1, N_r2 at the given spectra: the
+ * reference's curr_func + wnonl_func + r1nonl_func + r2nonl_func
+ * (Qsolver.cuh:166-312), fused. Inputs are not modified. */
+qaf_status qaf_nonlinear(qaf_mesh* mesh, const qaf_params* p, const void* w, const void* r1, const void* r2,
+                         void* w_nl, void* r1_nl, void* r2_nl, void* stream);
+/* nsteps steps of the chosen integrator on the spectral state (w, r1, r2),
+ * in place, each ending with dealias and old <- new: the loop of
+ * InertialFriction/friction/friction.cu:212-259, fused into two kernels per
+ * RK stage. Asynchronous on `stream`. */
+qaf_status qaf_step(qaf_mesh* mesh, const qaf_params* p, qaf_integrator integ, void* w, void* r1, void* r2,
+                    int nsteps, void* stream);
+/* The same with the state and result in HOST memory: copies in, steps, copies
+ * out, synchronises. */
+qaf_status qaf_step_host(qaf_mesh* mesh, const qaf_params* p, qaf_integrator integ, void* w, void* r1, void* r2,
+                         int nsteps);
+/* Diagnostics of the last qaf_step on this mesh (its final state), after the
+ * stream has been synchronised: out[0] = total energy sum 0.5 (u^2+v^2) dx dy /
+ * (Lx Ly) (post_process/postprocess.cu:54-65,158-161), out[1] = enstrophy
+ * 0.5 <w^2>. Returns QAF_ERR_NONFINITE if a step produced Inf/NaN. */
+qaf_status qaf_last_diagnostics(qaf_mesh* mesh, double out[2]);
+/* Synchronises `stream` and reports whether any step since the last call
+ * produced a non-finite value (the reference's NaN check, friction.cu:280). */
+qaf_status qaf_check_finite(qaf_mesh* mesh, void* stream);
+
+/* ---- resident state -------------------------------------------------------
+ * The reference keeps its state on the device for the whole run and touches
+ * the host only for periodic dumps (friction.cu:212-282). The same here: load
+ * a spectral state into the mesh's own buffers once, advance it as often as
+ * needed, store it when a snapshot is wanted. qaf_step = load + advance + store. */
+qaf_status qaf_state_load(qaf_mesh* mesh, const void* w, const void* r1, const void* r2, void* stream);
+qaf_status qaf_state_advance(qaf_mesh* mesh, const qaf_params* p, qaf_integrator integ, int nsteps, void* stream);
+qaf_status qaf_state_store(qaf_mesh* mesh, void* w, void* r1, void* r2, void* stream);
+/* Advance the resident state by nsteps steps with CUDA events recorded on
+ * `stream` around every row and column kernel; out_ms[0] / out_ms[1] = mean
+ * duration of one row / one column kernel, out_ms[2] = their launch count.
+ * Synchronises `stream`. (Measurement support for the roofline figures.) */
+qaf_status qaf_state_advance_timed(qaf_mesh* mesh, const qaf_params* p, qaf_integrator integ, int nsteps,
+                                   double out_ms[3], void* stream);
+/* Number of kernels this mesh has launched so far. */
+uint64_t qaf_launch_count(const qaf_mesh* mesh);
+
+/* ---- diagnostics of a spectral state (post_process/) --------------------- */
+/* energy and enstrophy as in qaf_last_diagnostics, and the shell spectrum
+ * E(k_s), k_s = s dk, s < nshells, dk = 2 pi / Lx (EnergySpec.cu:81-96),
+ * written to host memory; `w` is a device spectrum */
+qaf_status qaf_diagnostics(qaf_mesh* mesh, const void* w, double* energy, double* enstrophy, double* spectrum,
+                           int nshells, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QAF_H */

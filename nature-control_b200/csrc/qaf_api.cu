@@ -1,0 +1,771 @@
+// qaf_api.cu — the C ABI of include/qaf.h: meshes, workspaces, launch
+// configuration per grid size and precision, and the step driver.
+#include "qaf.h"
+#include "qaf_kernels.cuh"
+#include "qaf_ops.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace qaf;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+qaf_status fail(qaf_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+#define QAF_CUDA(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return fail(QAF_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+#define QAF_TRY(expr)                  \
+    do {                               \
+        qaf_status s_ = (expr);        \
+        if (s_ != QAF_OK) return s_;   \
+    } while (0)
+
+bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+constexpr int kMinN = 16, kMaxN = 1024;
+
+// ---------------------------------------------------------------------------
+// launch configuration per (precision, N)
+// ---------------------------------------------------------------------------
+template <typename real, int N>
+struct Cfg {
+    static constexpr int H = N / 2;
+    static constexpr int W = (sizeof(real) == 4 ? 8 : 4) < H ? (sizeof(real) == 4 ? 8 : 4) : H;  // columns per CTA
+    static constexpr int EC = 8;                                                              // column FFT values/thread
+    static constexpr int ER = (sizeof(real) == 4 ? 8 : 4) < H ? (sizeof(real) == 4 ? 8 : 4) : H;  // row FFT values/thread
+    static constexpr int TEAM_R = H / ER;
+    static constexpr int ROWS = (TEAM_R >= 128) ? 1 : (128 / TEAM_R <= N ? 128 / TEAM_R : N);
+    static constexpr int COL_THREADS = W * (N / EC);
+    static constexpr int ROW_THREADS = ROWS * TEAM_R;
+    static constexpr size_t COL_SMEM = (size_t)(W * N + 2 * N) * sizeof(cplx<real>);
+    static constexpr size_t ROW_SMEM = (size_t)ROWS * H * sizeof(cplx<real>);
+    static constexpr int COL_BLOCKS = 3 * (H / W) + 3;
+    static constexpr int ROW_BLOCKS = N / ROWS;
+};
+
+template <typename real>
+struct Workspace {
+    int N = 0;
+    cplx<real>* block = nullptr;  // one allocation for everything below
+    cplx<real>* old_m[3];
+    cplx<real>* old_n[3];
+    cplx<real>* acc_m[3];
+    cplx<real>* acc_n[3];
+    cplx<real>* Y;
+    cplx<real>* D;
+    cplx<real>* G;
+    cplx<real>* Ed;
+    cplx<real>* T;     // transform scratch
+    cplx<real>* tw;
+    real* ex;
+    real* ey;
+    double* diag;      // [0] energy sum, [1] enstrophy sum, [2..] spectrum shells (scratch)
+    unsigned* flags;
+    double cached[5] = {NAN, NAN, NAN, NAN, NAN};   // dt, re, rf, q_lin, unused -> IF tables valid for
+    real e0[4];
+};
+
+size_t align_up(size_t x) { return (x + 31) & ~size_t(31); }
+
+}  // namespace
+
+struct qaf_mesh {
+    qaf_mesh_desc desc;
+    int nxh;
+    double dkx, dky;
+    Workspace<float> wf;
+    Workspace<double> wd;
+    int device;
+    bool loaded = false;    // the resident state holds a loaded spectral state
+    bool y_valid = false;   // the Y/D arrays hold the inverse transforms of that state
+    uint64_t launches = 0;
+};
+
+namespace {
+
+template <typename real>
+Workspace<real>& ws(qaf_mesh* m);
+template <> Workspace<float>& ws<float>(qaf_mesh* m) { return m->wf; }
+template <> Workspace<double>& ws<double>(qaf_mesh* m) { return m->wd; }
+
+template <typename real>
+qaf_status ensure_ws(qaf_mesh* m) {
+    Workspace<real>& w = ws<real>(m);
+    if (w.block) return QAF_OK;
+    const int N = m->desc.nx, H = N / 2;
+    const size_t plane = (size_t)N * H;
+    // element counts (complex)
+    size_t off = 0;
+    auto take = [&](size_t n) { size_t o = off; off += align_up(n); return o; };
+    size_t o_old_m[3], o_old_n[3], o_acc_m[3], o_acc_n[3];
+    for (int f = 0; f < 3; ++f) { o_old_m[f] = take(plane); o_old_n[f] = take(N); }
+    for (int f = 0; f < 3; ++f) { o_acc_m[f] = take(plane); o_acc_n[f] = take(N); }
+    size_t oY = take(NY * plane), oD = take((size_t)PF_COUNT * N), oG = take(NG * plane), oE = take((size_t)NE * N);
+    size_t oT = take(plane), otw = take(N);
+    // real tables stored in complex slots
+    size_t oex = take((4 * (H + 1) + 1) / 2 + 1), oey = take((4 * N + 1) / 2 + 1);
+    size_t odiag = take((4 + 512 + 513) * sizeof(double) / sizeof(cplx<real>) + 1);
+    size_t oflags = take(1);
+    cplx<real>* b = nullptr;
+    cudaError_t e = cudaMalloc((void**)&b, off * sizeof(cplx<real>));
+    if (e != cudaSuccess) return fail(QAF_ERR_ALLOC, std::string("workspace cudaMalloc: ") + cudaGetErrorString(e));
+    w.block = b;
+    w.N = N;
+    for (int f = 0; f < 3; ++f) {
+        w.old_m[f] = b + o_old_m[f]; w.old_n[f] = b + o_old_n[f];
+        w.acc_m[f] = b + o_acc_m[f]; w.acc_n[f] = b + o_acc_n[f];
+    }
+    w.Y = b + oY; w.D = b + oD; w.G = b + oG; w.Ed = b + oE; w.T = b + oT; w.tw = b + otw;
+    w.ex = reinterpret_cast<real*>(b + oex);
+    w.ey = reinterpret_cast<real*>(b + oey);
+    w.diag = reinterpret_cast<double*>(b + odiag);
+    w.flags = reinterpret_cast<unsigned*>(b + oflags);
+    // twiddles exp(-2 pi i m / N) from long double
+    std::vector<cplx<real>> tw(N);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < N; ++k) {
+        long double a = -2.0L * pi * (long double)k / (long double)N;
+        tw[k] = mk<real>((real)cosl(a), (real)sinl(a));
+    }
+    QAF_CUDA(cudaMemcpy(w.tw, tw.data(), N * sizeof(cplx<real>), cudaMemcpyHostToDevice));
+    QAF_CUDA(cudaMemset(w.flags, 0, sizeof(unsigned)));
+    QAF_CUDA(cudaMemset(w.diag, 0, 2 * sizeof(double)));
+    return QAF_OK;
+}
+
+// Separable integrating factors: exp(L dt) with L_w = (-kx^2 - ky^2 - Rf)/Re
+// and L_Q = -kx^2 - ky^2 + q_lin factor into exp(-c kx^2 dt) exp(-c ky^2 dt) exp(c0 dt).
+template <typename real>
+qaf_status ensure_if(qaf_mesh* m, const qaf_params* p, cudaStream_t st) {
+    Workspace<real>& w = ws<real>(m);
+    if (w.cached[0] == p->dt && w.cached[1] == p->re && w.cached[2] == p->rf && w.cached[3] == p->q_lin) return QAF_OK;
+    const int N = m->desc.nx, H = N / 2;
+    std::vector<real> ex(4 * (H + 1)), ey(4 * N);
+    const double steps[4] = {p->dt, 0.5 * p->dt, p->dt, 0.5 * p->dt};
+    const double visc[4] = {1.0 / p->re, 1.0 / p->re, 1.0, 1.0};
+    for (int c = 0; c < 4; ++c) {
+        for (int i = 0; i <= H; ++i) {
+            long double kx = (long double)m->dkx * i;
+            ex[c * (H + 1) + i] = (real)expl(-(long double)visc[c] * kx * kx * (long double)steps[c]);
+        }
+        for (int j = 0; j < N; ++j) {
+            long double ky = (long double)m->dky * (j < N / 2 + 1 ? j : j - N);
+            ey[c * N + j] = (real)expl(-(long double)visc[c] * ky * ky * (long double)steps[c]);
+        }
+    }
+    w.e0[0] = (real)expl(-(long double)p->rf / p->re * p->dt);
+    w.e0[1] = (real)expl(-(long double)p->rf / p->re * p->dt * 0.5L);
+    w.e0[2] = (real)expl((long double)p->q_lin * p->dt);
+    w.e0[3] = (real)expl((long double)p->q_lin * p->dt * 0.5L);
+    QAF_CUDA(cudaMemcpyAsync(w.ex, ex.data(), ex.size() * sizeof(real), cudaMemcpyHostToDevice, st));
+    QAF_CUDA(cudaMemcpyAsync(w.ey, ey.data(), ey.size() * sizeof(real), cudaMemcpyHostToDevice, st));
+    QAF_CUDA(cudaStreamSynchronize(st));   // host vectors go out of scope
+    w.cached[0] = p->dt; w.cached[1] = p->re; w.cached[2] = p->rf; w.cached[3] = p->q_lin;
+    return QAF_OK;
+}
+
+template <typename real>
+StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
+    Workspace<real>& w = ws<real>(m);
+    const int N = m->desc.nx, nxh = N / 2 + 1;
+    StageArgs<real> a;
+    std::memset(&a, 0, sizeof(a));
+    a.dkx = (real)m->dkx; a.dky = (real)m->dky;
+    a.lambda = (real)p->lambda; a.ce = (real)(1.0 / (p->er * p->re)); a.alpha = (real)p->alpha;
+    a.alpha_field = reinterpret_cast<const real*>(p->alpha_field);
+    a.dt = (real)p->dt; a.advect = p->advect_omega ? 1 : 0;
+    a.kx_keep = (nxh - 1) * 2 / 3;
+    a.ky_lo = N / 3;
+    a.ky_hi = N - N / 3 + 1;
+    for (int f = 0; f < 3; ++f) {
+        a.old_m[f] = w.old_m[f]; a.old_n[f] = w.old_n[f]; a.acc_m[f] = w.acc_m[f]; a.acc_n[f] = w.acc_n[f];
+        a.nl_m[f] = w.acc_m[f]; a.nl_n[f] = w.acc_n[f];
+    }
+    a.Y = w.Y; a.D = w.D; a.G = w.G; a.Ed = w.Ed; a.tw = w.tw; a.ex = w.ex; a.ey = w.ey;
+    for (int c = 0; c < 4; ++c) a.e0[c] = w.e0[c];
+    a.diag = w.diag; a.flags = w.flags;
+    return a;
+}
+
+// ---------------------------------------------------------------------------
+// per-size launchers
+// ---------------------------------------------------------------------------
+template <typename real, int N>
+struct Launch {
+    using C = Cfg<real, N>;
+    static qaf_status setup() {
+        static bool done = false;
+        if (done) return QAF_OK;
+        QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::ROW_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(col_ifft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(col_fft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
+        done = true;
+        return QAF_OK;
+    }
+    static void col(const StageArgs<real>& a, cudaStream_t st) {
+        col_kernel<real, N, C::W, C::EC><<<C::COL_BLOCKS, C::COL_THREADS, C::COL_SMEM, st>>>(a);
+    }
+    static void row(const StageArgs<real>& a, cudaStream_t st) {
+        row_kernel<real, N, C::ER, C::ROWS><<<C::ROW_BLOCKS, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
+    }
+    static void bwd(const cplx<real>* spec, cplx<real>* T, real* phys, const cplx<real>* tw, cudaStream_t st) {
+        col_ifft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COL_THREADS, C::COL_SMEM, st>>>(spec, T, tw);
+        row_c2r_kernel<real, N, C::ER, C::ROWS><<<C::ROW_BLOCKS, C::ROW_THREADS, C::ROW_SMEM, st>>>(T, phys, tw);
+    }
+    static void fwd(const real* phys, cplx<real>* T, cplx<real>* spec, const cplx<real>* tw, cudaStream_t st) {
+        row_r2c_kernel<real, N, C::ER, C::ROWS><<<C::ROW_BLOCKS, C::ROW_THREADS, C::ROW_SMEM, st>>>(phys, T, tw);
+        col_fft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COL_THREADS, C::COL_SMEM, st>>>(T, spec, tw);
+    }
+};
+
+// Calls F::template run<real, N>(args...) for the mesh's precision and size.
+template <class F, class... A>
+qaf_status dispatch(const qaf_mesh* m, A&&... args) {
+    const int N = m->desc.nx;
+    const bool f64 = m->desc.dtype == QAF_F64;
+#define QAF_CASE(n)                                                                       \
+    case n:                                                                               \
+        return f64 ? F::template run<double, n>(std::forward<A>(args)...)                \
+                   : F::template run<float, n>(std::forward<A>(args)...);
+    switch (N) {
+        QAF_CASE(16) QAF_CASE(32) QAF_CASE(64) QAF_CASE(128) QAF_CASE(256) QAF_CASE(512) QAF_CASE(1024)
+        default: break;
+    }
+#undef QAF_CASE
+    return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size (need nx == ny, a power of two in [16, 1024])");
+}
+
+qaf_status check_mesh(const qaf_mesh* m) {
+    if (!m) return fail(QAF_ERR_INVALID, "null mesh");
+    return QAF_OK;
+}
+
+size_t spec_elems(const qaf_mesh* m) { return (size_t)m->nxh * m->desc.ny; }
+size_t phys_elems(const qaf_mesh* m) { return (size_t)m->desc.nx * m->desc.ny; }
+size_t real_bytes(const qaf_mesh* m) { return m->desc.dtype == QAF_F64 ? 8 : 4; }
+
+Geo geo(const qaf_mesh* m) { return Geo{m->desc.nx, m->desc.ny, m->nxh, m->dkx, m->dky}; }
+int grid_for(size_t n) { size_t g = (n + 255) / 256; return (int)(g > 148 * 16 ? 148 * 16 : (g < 1 ? 1 : g)); }
+
+qaf_status post_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(QAF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return QAF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// operations
+// ---------------------------------------------------------------------------
+struct OpBwd {
+    template <typename real, int N>
+    static qaf_status run(qaf_mesh* m, const void* spec, void* phys, cudaStream_t st) {
+        QAF_TRY(ensure_ws<real>(m));
+        QAF_TRY((Launch<real, N>::setup()));
+        Workspace<real>& w = ws<real>(m);
+        Launch<real, N>::bwd(reinterpret_cast<const cplx<real>*>(spec), w.T, reinterpret_cast<real*>(phys), w.tw, st);
+        return post_launch("BwdTrans");
+    }
+};
+
+struct OpFwd {
+    template <typename real, int N>
+    static qaf_status run(qaf_mesh* m, const void* phys, void* spec, cudaStream_t st) {
+        QAF_TRY(ensure_ws<real>(m));
+        QAF_TRY((Launch<real, N>::setup()));
+        Workspace<real>& w = ws<real>(m);
+        Launch<real, N>::fwd(reinterpret_cast<const real*>(phys), w.T, reinterpret_cast<cplx<real>*>(spec), w.tw, st);
+        return post_launch("FwdTrans");
+    }
+};
+
+template <typename real>
+void to_internal(qaf_mesh* m, const void* ref, int f, cudaStream_t st) {
+    Workspace<real>& w = ws<real>(m);
+    ref_to_internal<real><<<grid_for(spec_elems(m)), 256, 0, st>>>(reinterpret_cast<const cplx<real>*>(ref), w.old_m[f], w.old_n[f], m->desc.nx);
+}
+
+template <typename real>
+void from_internal(qaf_mesh* m, cplx<real>* mm, cplx<real>* nq, void* ref, cudaStream_t st) {
+    internal_to_ref<real><<<grid_for(spec_elems(m)), 256, 0, st>>>(mm, nq, reinterpret_cast<cplx<real>*>(ref), m->desc.nx);
+}
+
+struct OpNonlinear {
+    template <typename real, int N>
+    static qaf_status run(qaf_mesh* m, const qaf_params* p, const void* const* in, void* const* out, void* phys_out,
+                          cudaStream_t st) {
+        QAF_TRY(ensure_ws<real>(m));
+        QAF_TRY((Launch<real, N>::setup()));
+        Workspace<real>& w = ws<real>(m);
+        for (int f = 0; f < 3; ++f) to_internal<real>(m, in[f], f, st);
+        m->loaded = true;      // the nonlinear evaluation reuses the state buffers
+        m->y_valid = false;
+        m->launches += 9;
+        StageArgs<real> a = make_args<real>(m, p);
+        a.phys_out = static_cast<real*>(phys_out);
+        a.mode = MODE_PROLOGUE; a.do_inverse = 1;
+        Launch<real, N>::col(a, st);
+        Launch<real, N>::row(a, st);
+        a.mode = MODE_NONL; a.do_inverse = 0;
+        Launch<real, N>::col(a, st);
+        for (int f = 0; f < 3; ++f) from_internal<real>(m, w.acc_m[f], w.acc_n[f], out[f], st);
+        return post_launch("qaf_nonlinear");
+    }
+};
+
+struct OpLoad {
+    template <typename real, int N>
+    static qaf_status run(qaf_mesh* m, void* const* state, cudaStream_t st) {
+        QAF_TRY(ensure_ws<real>(m));
+        for (int f = 0; f < 3; ++f) to_internal<real>(m, state[f], f, st);
+        m->launches += 3;
+        m->loaded = true;
+        m->y_valid = false;
+        return post_launch("qaf_state_load");
+    }
+};
+
+struct OpStore {
+    template <typename real, int N>
+    static qaf_status run(qaf_mesh* m, void* const* state, cudaStream_t st) {
+        Workspace<real>& w = ws<real>(m);
+        for (int f = 0; f < 3; ++f) from_internal<real>(m, w.old_m[f], w.old_n[f], state[f], st);
+        m->launches += 3;
+        return post_launch("qaf_state_store");
+    }
+};
+
+// Events around every row/column launch when `ev` is given (timed variant).
+struct KernelTimer {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;    // 0 row, 1 column
+};
+
+struct OpAdvance {
+    template <typename real, int N>
+    static qaf_status run(qaf_mesh* m, const qaf_params* p, int integ, int nsteps, bool final_inverse, KernelTimer* timer,
+                          cudaStream_t st) {
+        QAF_TRY(ensure_ws<real>(m));
+        QAF_TRY((Launch<real, N>::setup()));
+        QAF_TRY(ensure_if<real>(m, p, st));
+        Workspace<real>& w = ws<real>(m);
+        StageArgs<real> a = make_args<real>(m, p);
+        a.integrator = integ;
+        const int nst = integ == QAF_IFRK4 ? 4 : (integ == QAF_IFRK2 ? 2 : 1);
+        auto launch = [&](int kind) {
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            if (timer) {
+                cudaEventCreate(&e0); cudaEventCreate(&e1);
+                cudaEventRecord(e0, st);
+            }
+            if (kind == 0) Launch<real, N>::row(a, st); else Launch<real, N>::col(a, st);
+            if (timer) {
+                cudaEventRecord(e1, st);
+                timer->ev.push_back(e0); timer->ev.push_back(e1); timer->kind.push_back(kind);
+            }
+            m->launches += 1;
+        };
+        if (!m->y_valid) {
+            a.mode = MODE_PROLOGUE; a.do_inverse = 1;
+            Launch<real, N>::col(a, st);
+            m->launches += 1;
+        }
+        a.mode = MODE_STAGE;
+        for (int s = 0; s < nsteps; ++s) {
+            const bool last_step = s == nsteps - 1;
+            if (last_step) {
+                QAF_CUDA(cudaMemsetAsync(w.diag, 0, 2 * sizeof(double), st));
+                m->launches += 1;
+            }
+            for (int k = 1; k <= nst; ++k) {
+                a.stage = k;
+                a.last_stage = k == nst;
+                a.do_inverse = !(last_step && k == nst && !final_inverse);
+                a.diag = (last_step && k == nst) ? w.diag : nullptr;
+                launch(0);
+                launch(1);
+            }
+        }
+        m->y_valid = final_inverse;
+        return post_launch("qaf_state_advance");
+    }
+};
+
+template <typename real>
+qaf_status diag_impl(qaf_mesh* m, const void* wspec, double* energy, double* enstrophy, double* spectrum, int nshells,
+                     cudaStream_t st) {
+    QAF_TRY(ensure_ws<real>(m));
+    Workspace<real>& w = ws<real>(m);
+    if (nshells > 512) return fail(QAF_ERR_INVALID, "at most 512 spectrum shells");
+    QAF_CUDA(cudaMemsetAsync(w.diag + 2, 0, (2 + (size_t)(nshells > 0 ? nshells : 0)) * sizeof(double), st));
+    // shell bounds k_0 = 0, k_{s+1} = k_s + dk, by repeated addition as the post-processor does
+    std::vector<double> bounds(nshells + 1 > 0 ? nshells + 1 : 1, 0.0);
+    const double dk = 2 * M_PI / m->desc.lx;
+    for (int s = 1; s <= nshells; ++s) bounds[s] = bounds[s - 1] + dk;
+    double* dbounds = w.diag + 4 + 512;
+    QAF_CUDA(cudaMemcpyAsync(dbounds, bounds.data(), bounds.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    diag_kernel<real><<<grid_for(spec_elems(m)), 256, 0, st>>>(geo(m), reinterpret_cast<const cplx<real>*>(wspec),
+                                                               w.diag + 2, dbounds, nshells);
+    QAF_TRY(post_launch("qaf_diagnostics"));
+    std::vector<double> h(2 + (nshells > 0 ? nshells : 0));
+    QAF_CUDA(cudaMemcpyAsync(h.data(), w.diag + 2, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    QAF_CUDA(cudaStreamSynchronize(st));   // also keeps `bounds` alive until the copy is done
+    const double n4 = (double)m->desc.nx * m->desc.ny * (double)m->desc.nx * m->desc.ny;
+    if (energy) *energy = 0.5 * h[0] / n4;
+    if (enstrophy) *enstrophy = 0.5 * h[1] / n4;
+    if (spectrum && nshells > 0) {
+        const double dk = 2 * M_PI / m->desc.lx;
+        const double norm = 2.0 * dk * n4;
+        for (int s = 0; s < nshells; ++s) spectrum[s] = h[2 + s] / norm;
+    }
+    return QAF_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* qaf_version(void) { return "qaf-b200 0.1 (sm_100a)"; }
+const char* qaf_last_error(void) { return g_last_error.c_str(); }
+
+int qaf_supported(int n, qaf_dtype dtype) {
+    return (dtype == QAF_F32 || dtype == QAF_F64) && pow2(n) && n >= kMinN && n <= kMaxN;
+}
+
+qaf_status qaf_mesh_create(const qaf_mesh_desc* desc, qaf_mesh** out) {
+    if (!desc || !out) return fail(QAF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (desc->nx < 4 || desc->ny < 4 || desc->nx % 2) return fail(QAF_ERR_INVALID, "nx, ny must be >= 4 and nx even");
+    if (!(desc->lx > 0) || !(desc->ly > 0)) return fail(QAF_ERR_INVALID, "lx, ly must be positive");
+    if (desc->dtype != QAF_F32 && desc->dtype != QAF_F64) return fail(QAF_ERR_INVALID, "bad dtype");
+    qaf_mesh* m = new qaf_mesh();
+    m->desc = *desc;
+    m->nxh = desc->nx / 2 + 1;
+    m->dkx = 2 * M_PI / desc->lx;   // waveinit, Mesh.cuh:6-21
+    m->dky = 2 * M_PI / desc->ly;
+    cudaGetDevice(&m->device);
+    *out = m;
+    return QAF_OK;
+}
+
+qaf_status qaf_mesh_destroy(qaf_mesh* m) {
+    if (!m) return QAF_OK;
+    if (m->wf.block) cudaFree(m->wf.block);
+    if (m->wd.block) cudaFree(m->wd.block);
+    delete m;
+    return QAF_OK;
+}
+
+qaf_status qaf_mesh_sizes(const qaf_mesh* m, size_t* phys_bytes, size_t* spec_bytes) {
+    QAF_TRY(check_mesh(m));
+    if (phys_bytes) *phys_bytes = phys_elems(m) * real_bytes(m);
+    if (spec_bytes) *spec_bytes = spec_elems(m) * 2 * real_bytes(m);
+    return QAF_OK;
+}
+
+qaf_status qaf_field_alloc(const qaf_mesh* m, void** phys, void** spec) {
+    QAF_TRY(check_mesh(m));
+    if (phys) { *phys = nullptr; QAF_CUDA(cudaMalloc(phys, phys_elems(m) * real_bytes(m))); }
+    if (spec) { *spec = nullptr; QAF_CUDA(cudaMalloc(spec, spec_elems(m) * 2 * real_bytes(m))); }
+    return QAF_OK;
+}
+
+qaf_status qaf_field_free(void* phys, void* spec) {
+    if (phys) cudaFree(phys);
+    if (spec) cudaFree(spec);
+    return QAF_OK;
+}
+
+qaf_status qaf_mesh_tables(const qaf_mesh* m, void* kx, void* ky, void* k2, void* cutoff) {
+    QAF_TRY(check_mesh(m));
+    const int nxh = m->nxh, ny = m->desc.ny;
+    const bool f64 = m->desc.dtype == QAF_F64;
+    for (int i = 0; i < nxh; ++i)
+        for (int j = 0; j < ny; ++j) {
+            const size_t idx = i + (size_t)j * nxh;
+            const double kyv = (j < ny / 2 + 1) ? 2 * M_PI / m->desc.ly * j : 2 * M_PI / m->desc.ly * (j - ny);
+            const double kxv = 2 * M_PI / m->desc.lx * i;
+            const double k2v = kxv * kxv + kyv * kyv;
+            const double cut = ((i < (nxh - 1) * 2 / 3 + 1) && ((j < ny / 3 + 1) || ((ny - j) < ny / 3))) ? 1.0 : 0.0;
+            const double vals[4] = {kxv, kyv, k2v, cut};
+            void* dst[4] = {kx, ky, k2, cutoff};
+            for (int q = 0; q < 4; ++q) {
+                if (!dst[q]) continue;
+                if (f64) static_cast<double*>(dst[q])[idx] = vals[q];
+                else static_cast<float*>(dst[q])[idx] = (float)vals[q];
+            }
+        }
+    return QAF_OK;
+}
+
+qaf_status qaf_bwd_trans(qaf_mesh* m, const void* spec, void* phys, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!spec || !phys) return fail(QAF_ERR_INVALID, "null pointer");
+    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "transforms need nx == ny");
+    return dispatch<OpBwd>(m, m, spec, phys, (cudaStream_t)stream);
+}
+
+qaf_status qaf_fwd_trans(qaf_mesh* m, const void* phys, void* spec, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!spec || !phys) return fail(QAF_ERR_INVALID, "null pointer");
+    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "transforms need nx == ny");
+    return dispatch<OpFwd>(m, m, phys, spec, (cudaStream_t)stream);
+}
+
+#define QAF_BY_DTYPE(m, KERNEL_F32, KERNEL_F64) \
+    do { if ((m)->desc.dtype == QAF_F64) { KERNEL_F64; } else { KERNEL_F32; } } while (0)
+
+qaf_status qaf_symmetrize(qaf_mesh* m, void* spec, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!spec) return fail(QAF_ERR_INVALID, "null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    QAF_BY_DTYPE(m, (symmetrize_kernel<float><<<grid_for(m->desc.ny), 256, 0, st>>>(geo(m), (cplx<float>*)spec)),
+                    (symmetrize_kernel<double><<<grid_for(m->desc.ny), 256, 0, st>>>(geo(m), (cplx<double>*)spec)));
+    return post_launch("qaf_symmetrize");
+}
+
+static qaf_status unary(qaf_mesh* m, int op, const void* in, void* out, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!in || !out) return fail(QAF_ERR_INVALID, "null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    int g = grid_for(spec_elems(m));
+    QAF_BY_DTYPE(m, (spec_unary_kernel<float><<<g, 256, 0, st>>>(geo(m), op, (const cplx<float>*)in, (cplx<float>*)out)),
+                    (spec_unary_kernel<double><<<g, 256, 0, st>>>(geo(m), op, (const cplx<double>*)in, (cplx<double>*)out)));
+    return post_launch("spectral operator");
+}
+
+qaf_status qaf_xderiv(qaf_mesh* m, const void* in, void* out, void* stream) { return unary(m, 0, in, out, stream); }
+qaf_status qaf_yderiv(qaf_mesh* m, const void* in, void* out, void* stream) { return unary(m, 1, in, out, stream); }
+qaf_status qaf_laplacian(qaf_mesh* m, const void* in, void* out, void* stream) { return unary(m, 2, in, out, stream); }
+
+qaf_status qaf_vel(qaf_mesh* m, const void* w, void* u, void* v, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!w || !u || !v) return fail(QAF_ERR_INVALID, "null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    int g = grid_for(spec_elems(m));
+    QAF_BY_DTYPE(m, (vel_kernel<float><<<g, 256, 0, st>>>(geo(m), (const cplx<float>*)w, (cplx<float>*)u, (cplx<float>*)v)),
+                    (vel_kernel<double><<<g, 256, 0, st>>>(geo(m), (const cplx<double>*)w, (cplx<double>*)u, (cplx<double>*)v)));
+    return post_launch("qaf_vel");
+}
+
+qaf_status qaf_dealias(qaf_mesh* m, void* spec, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!spec) return fail(QAF_ERR_INVALID, "null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    int g = grid_for(spec_elems(m));
+    QAF_BY_DTYPE(m, (dealias_kernel<float><<<g, 256, 0, st>>>(geo(m), (cplx<float>*)spec)),
+                    (dealias_kernel<double><<<g, 256, 0, st>>>(geo(m), (cplx<double>*)spec)));
+    return post_launch("qaf_dealias");
+}
+
+qaf_status qaf_if_tables(qaf_mesh* m, const qaf_params* p, int which, void* IF, void* IFh, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!p || !IF || !IFh || (which != 0 && which != 1)) return fail(QAF_ERR_INVALID, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int g = grid_for(spec_elems(m));
+    QAF_BY_DTYPE(m, (if_table_kernel<float><<<g, 256, 0, st>>>(geo(m), which, p->re, p->rf, p->q_lin, p->dt, (float*)IF, (float*)IFh)),
+                    (if_table_kernel<double><<<g, 256, 0, st>>>(geo(m), which, p->re, p->rf, p->q_lin, p->dt, (double*)IF, (double*)IFh)));
+    return post_launch("qaf_if_tables");
+}
+
+qaf_status qaf_integrate(qaf_mesh* m, qaf_integrator integ, int stage, const void* old_spec, void* curr_spec,
+                         void* new_spec, const void* nonl_spec, const void* IF, const void* IFh, double dt, void* stream) {
+    QAF_TRY(check_mesh(m));
+    const int max_stage = integ == QAF_IFRK4 ? 4 : (integ == QAF_IFRK2 ? 2 : 1);
+    const int min_stage = integ == QAF_IFE ? 1 : 0;
+    if (stage < min_stage || stage > max_stage) return fail(QAF_ERR_INVALID, "bad stage for this integrator");
+    if (!old_spec || !new_spec || !IF || !IFh || (stage > 0 && !nonl_spec) || (integ != QAF_IFE && !curr_spec))
+        return fail(QAF_ERR_INVALID, "null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t n = spec_elems(m);
+    int g = grid_for(n);
+    QAF_BY_DTYPE(m,
+        (integrate_kernel<float><<<g, 256, 0, st>>>(n, (int)integ, stage, (const cplx<float>*)old_spec, (cplx<float>*)curr_spec,
+            (cplx<float>*)new_spec, (const cplx<float>*)nonl_spec, (const float*)IF, (const float*)IFh, (float)dt)),
+        (integrate_kernel<double><<<g, 256, 0, st>>>(n, (int)integ, stage, (const cplx<double>*)old_spec, (cplx<double>*)curr_spec,
+            (cplx<double>*)new_spec, (const cplx<double>*)nonl_spec, (const double*)IF, (const double*)IFh, dt)));
+    return post_launch("qaf_integrate");
+}
+
+static qaf_status check_params(const qaf_params* p) {
+    if (!p) return fail(QAF_ERR_INVALID, "null params");
+    if (!(p->re > 0) || !(p->er > 0)) return fail(QAF_ERR_INVALID, "re and er must be positive");
+    if (!std::isfinite(p->dt) || !std::isfinite(p->lambda) || !std::isfinite(p->rf) || !std::isfinite(p->alpha) ||
+        !std::isfinite(p->q_lin))
+        return fail(QAF_ERR_INVALID, "non-finite parameter");
+    return QAF_OK;
+}
+
+qaf_status qaf_nonlinear_dbg(qaf_mesh* m, const qaf_params* p, const void* w, const void* r1, const void* r2,
+                             void* w_nl, void* r1_nl, void* r2_nl, void* phys_out, void* stream);
+
+qaf_status qaf_nonlinear(qaf_mesh* m, const qaf_params* p, const void* w, const void* r1, const void* r2,
+                         void* w_nl, void* r1_nl, void* r2_nl, void* stream) {
+    return qaf_nonlinear_dbg(m, p, w, r1, r2, w_nl, r1_nl, r2_nl, nullptr, stream);
+}
+
+// qaf_nonlinear with an optional dump of the 13 physical fields of the row
+// pass (w r1 r2 u v du/dx du/dy+dv/dx Lap r1 Lap r2 S p11 p12 p21), for tests.
+qaf_status qaf_nonlinear_dbg(qaf_mesh* m, const qaf_params* p, const void* w, const void* r1, const void* r2,
+                             void* w_nl, void* r1_nl, void* r2_nl, void* phys_out, void* stream) {
+    QAF_TRY(check_mesh(m));
+    QAF_TRY(check_params(p));
+    if (!w || !r1 || !r2 || !w_nl || !r1_nl || !r2_nl) return fail(QAF_ERR_INVALID, "null pointer");
+    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "the fused path needs nx == ny");
+    const void* in[3] = {w, r1, r2};
+    void* out[3] = {w_nl, r1_nl, r2_nl};
+    return dispatch<OpNonlinear>(m, m, p, (const void* const*)in, (void* const*)out, phys_out, (cudaStream_t)stream);
+}
+
+static qaf_status check_advance(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, int nsteps) {
+    QAF_TRY(check_mesh(m));
+    QAF_TRY(check_params(p));
+    if (integ != QAF_IFE && integ != QAF_IFRK2 && integ != QAF_IFRK4) return fail(QAF_ERR_INVALID, "bad integrator");
+    if (nsteps < 0) return fail(QAF_ERR_INVALID, "nsteps < 0");
+    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "the fused path needs nx == ny");
+    return QAF_OK;
+}
+
+qaf_status qaf_state_load(qaf_mesh* m, const void* w, const void* r1, const void* r2, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!w || !r1 || !r2) return fail(QAF_ERR_INVALID, "null pointer");
+    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "the fused path needs nx == ny");
+    void* st[3] = {const_cast<void*>(w), const_cast<void*>(r1), const_cast<void*>(r2)};
+    return dispatch<OpLoad>(m, m, (void* const*)st, (cudaStream_t)stream);
+}
+
+qaf_status qaf_state_store(qaf_mesh* m, void* w, void* r1, void* r2, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!w || !r1 || !r2) return fail(QAF_ERR_INVALID, "null pointer");
+    if (!m->loaded) return fail(QAF_ERR_INVALID, "no state loaded on this mesh");
+    void* st[3] = {w, r1, r2};
+    return dispatch<OpStore>(m, m, (void* const*)st, (cudaStream_t)stream);
+}
+
+qaf_status qaf_state_advance(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, int nsteps, void* stream) {
+    QAF_TRY(check_advance(m, p, integ, nsteps));
+    if (!m->loaded) return fail(QAF_ERR_INVALID, "no state loaded on this mesh");
+    if (nsteps == 0) return QAF_OK;
+    return dispatch<OpAdvance>(m, m, p, (int)integ, nsteps, true, (KernelTimer*)nullptr, (cudaStream_t)stream);
+}
+
+qaf_status qaf_state_advance_timed(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, int nsteps, double out_ms[3],
+                                   void* stream) {
+    QAF_TRY(check_advance(m, p, integ, nsteps));
+    if (!m->loaded) return fail(QAF_ERR_INVALID, "no state loaded on this mesh");
+    if (!out_ms) return fail(QAF_ERR_INVALID, "null pointer");
+    KernelTimer timer;
+    qaf_status s = nsteps ? dispatch<OpAdvance>(m, m, p, (int)integ, nsteps, true, &timer, (cudaStream_t)stream) : QAF_OK;
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    double sum[2] = {0, 0};
+    int cnt[2] = {0, 0};
+    for (size_t k = 0; k < timer.kind.size(); ++k) {
+        float ms = 0;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, timer.ev[2 * k], timer.ev[2 * k + 1]);
+        sum[timer.kind[k]] += ms;
+        cnt[timer.kind[k]] += 1;
+    }
+    for (cudaEvent_t ev : timer.ev) cudaEventDestroy(ev);
+    if (s != QAF_OK) return s;
+    if (e != cudaSuccess) return fail(QAF_ERR_CUDA, std::string("qaf_state_advance_timed: ") + cudaGetErrorString(e));
+    out_ms[0] = cnt[0] ? sum[0] / cnt[0] : 0.0;
+    out_ms[1] = cnt[1] ? sum[1] / cnt[1] : 0.0;
+    out_ms[2] = (double)(cnt[0] + cnt[1]);
+    return QAF_OK;
+}
+
+uint64_t qaf_launch_count(const qaf_mesh* m) { return m ? m->launches : 0; }
+
+qaf_status qaf_step(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, void* w, void* r1, void* r2, int nsteps,
+                    void* stream) {
+    QAF_TRY(check_advance(m, p, integ, nsteps));
+    if (!w || !r1 || !r2) return fail(QAF_ERR_INVALID, "null pointer");
+    if (nsteps == 0) return QAF_OK;
+    void* st[3] = {w, r1, r2};
+    cudaStream_t s = (cudaStream_t)stream;
+    QAF_TRY(dispatch<OpLoad>(m, m, (void* const*)st, s));
+    QAF_TRY(dispatch<OpAdvance>(m, m, p, (int)integ, nsteps, false, (KernelTimer*)nullptr, s));
+    return dispatch<OpStore>(m, m, (void* const*)st, s);
+}
+
+qaf_status qaf_step_host(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, void* w, void* r1, void* r2,
+                         int nsteps) {
+    QAF_TRY(check_mesh(m));
+    if (!w || !r1 || !r2) return fail(QAF_ERR_INVALID, "null pointer");
+    const size_t bytes = spec_elems(m) * 2 * real_bytes(m);
+    void* d = nullptr;
+    QAF_CUDA(cudaMalloc(&d, 3 * bytes));
+    char* dc = static_cast<char*>(d);
+    void* host[3] = {w, r1, r2};
+    qaf_status s = QAF_OK;
+    for (int f = 0; f < 3 && s == QAF_OK; ++f) {
+        cudaError_t e = cudaMemcpy(dc + f * bytes, host[f], bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) s = fail(QAF_ERR_CUDA, std::string("H2D: ") + cudaGetErrorString(e));
+    }
+    if (s == QAF_OK) s = qaf_step(m, p, integ, dc, dc + bytes, dc + 2 * bytes, nsteps, nullptr);
+    for (int f = 0; f < 3 && s == QAF_OK; ++f) {
+        cudaError_t e = cudaMemcpy(host[f], dc + f * bytes, bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) s = fail(QAF_ERR_CUDA, std::string("D2H: ") + cudaGetErrorString(e));
+    }
+    cudaFree(d);
+    return s;
+}
+
+qaf_status qaf_last_diagnostics(qaf_mesh* m, double out[2]) {
+    QAF_TRY(check_mesh(m));
+    if (!out) return fail(QAF_ERR_INVALID, "null pointer");
+    double h[2] = {0, 0};
+    unsigned flags = 0;
+    if (m->desc.dtype == QAF_F64) {
+        if (!m->wd.block) return fail(QAF_ERR_INVALID, "no step has run on this mesh");
+        QAF_CUDA(cudaMemcpy(h, m->wd.diag, sizeof(h), cudaMemcpyDeviceToHost));
+        QAF_CUDA(cudaMemcpy(&flags, m->wd.flags, sizeof(flags), cudaMemcpyDeviceToHost));
+    } else {
+        if (!m->wf.block) return fail(QAF_ERR_INVALID, "no step has run on this mesh");
+        QAF_CUDA(cudaMemcpy(h, m->wf.diag, sizeof(h), cudaMemcpyDeviceToHost));
+        QAF_CUDA(cudaMemcpy(&flags, m->wf.flags, sizeof(flags), cudaMemcpyDeviceToHost));
+    }
+    const double n4 = (double)m->desc.nx * m->desc.ny * (double)m->desc.nx * m->desc.ny;
+    out[0] = 0.5 * h[1] / n4;   // energy: sum |w|^2 / k^2
+    out[1] = 0.5 * h[0] / n4;   // enstrophy: sum |w|^2
+    if (flags) return fail(QAF_ERR_NONFINITE, "a step produced a non-finite value");
+    return QAF_OK;
+}
+
+qaf_status qaf_check_finite(qaf_mesh* m, void* stream) {
+    QAF_TRY(check_mesh(m));
+    QAF_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    unsigned* fp = m->desc.dtype == QAF_F64 ? m->wd.flags : m->wf.flags;
+    if (!fp) return QAF_OK;
+    unsigned flags = 0;
+    QAF_CUDA(cudaMemcpy(&flags, fp, sizeof(flags), cudaMemcpyDeviceToHost));
+    QAF_CUDA(cudaMemset(fp, 0, sizeof(unsigned)));
+    if (flags) return fail(QAF_ERR_NONFINITE, "a step produced a non-finite value");
+    return QAF_OK;
+}
+
+qaf_status qaf_diagnostics(qaf_mesh* m, const void* w, double* energy, double* enstrophy, double* spectrum, int nshells,
+                           void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!w) return fail(QAF_ERR_INVALID, "null pointer");
+    if (m->desc.dtype == QAF_F64) return diag_impl<double>(m, w, energy, enstrophy, spectrum, nshells, (cudaStream_t)stream);
+    return diag_impl<float>(m, w, energy, enstrophy, spectrum, nshells, (cudaStream_t)stream);
+}
+
+}  // extern "C"

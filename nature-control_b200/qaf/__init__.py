@@ -1,0 +1,334 @@
+"""qaf — Python face of the B200 pseudo-spectral active-nematic solver.
+
+A thin ctypes binding of the C ABI in include/qaf.h (libqaf.so, built in this
+directory by ``nature-control_b200/build.py``). Device memory and streams come
+from PyTorch CUDA tensors; every computation runs in the library's CUDA
+kernels. There is no CPU fallback: without the built library, or without a
+GPU, the calls raise.
+
+The names follow the reference's header-only API (whpy/nature-control):
+``Mesh`` (Basic/Mesh.cuh:48-113), ``fwd_trans``/``bwd_trans`` (FwdTrans /
+BwdTrans, FldOp/QFldfuncs.cuh:45-55), ``xderiv``/``yderiv``/``laplacian``/
+``vel`` (:165-224), ``nonlinear`` (curr_func + wnonl_func + r1nonl_func +
+r2nonl_func, InertialFriction/friction/Qsolver.cuh:166-312), ``step`` (the
+IF-RK4 loop of InertialFriction/friction/friction.cu:212-259, and the IF-RK2 /
+IF-Euler integrators of TimeIntegration/).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqaf.so")
+
+F32, F64 = 0, 1
+IFE, IFRK2, IFRK4 = 0, 1, 2
+OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_NONFINITE, ERR_ALLOC = range(6)
+
+# Every symbol include/qaf.h declares (the tests check the library exports them).
+EXPORTS = [
+    "qaf_version", "qaf_last_error", "qaf_supported", "qaf_mesh_create", "qaf_mesh_destroy", "qaf_mesh_sizes",
+    "qaf_field_alloc", "qaf_field_free", "qaf_mesh_tables", "qaf_fwd_trans", "qaf_bwd_trans", "qaf_symmetrize",
+    "qaf_xderiv", "qaf_yderiv", "qaf_laplacian", "qaf_vel", "qaf_dealias", "qaf_if_tables", "qaf_integrate",
+    "qaf_nonlinear", "qaf_step", "qaf_step_host", "qaf_last_diagnostics", "qaf_check_finite", "qaf_diagnostics",
+    "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_state_advance_timed", "qaf_launch_count",
+]
+
+
+class QafError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"qaf status {status}: {msg}")
+        self.status = status
+
+
+class NonFiniteError(QafError):
+    pass
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("lx", ctypes.c_double), ("ly", ctypes.c_double),
+                ("dtype", ctypes.c_int)]
+
+
+class CParams(ctypes.Structure):
+    _fields_ = [("re", ctypes.c_double), ("er", ctypes.c_double), ("rf", ctypes.c_double),
+                ("lam", ctypes.c_double), ("alpha", ctypes.c_double), ("alpha_field", ctypes.c_void_p),
+                ("dt", ctypes.c_double), ("q_lin", ctypes.c_double), ("advect_omega", ctypes.c_int)]
+
+
+@dataclass
+class Params:
+    """Physical parameters (InertialFriction/friction/friction.cu:100-105 names)."""
+    re: float = 1.0
+    er: float = 1.0
+    rf: float = 0.1
+    lam: float = 0.1
+    alpha: float = 1.0
+    dt: float = 1e-3
+    q_lin: float = 1.0
+    advect_omega: int = 1
+    alpha_field: Optional[object] = field(default=None, repr=False)   # torch tensor (ny, nx) on the device
+
+    def c(self) -> CParams:
+        ptr = None
+        if self.alpha_field is not None:
+            ptr = self.alpha_field.data_ptr()
+        return CParams(self.re, self.er, self.rf, self.lam, self.alpha, ptr, self.dt, self.q_lin, self.advect_omega)
+
+
+_lib = None
+
+
+def lib():
+    """Load libqaf.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python nature-control_b200/build.py` "
+                              "(or __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, cp = ctypes.c_void_p, ctypes.c_int
+        L.qaf_version.restype = ctypes.c_char_p
+        L.qaf_last_error.restype = ctypes.c_char_p
+        L.qaf_supported.argtypes = [cp, cp]
+        L.qaf_mesh_create.argtypes = [ctypes.POINTER(MeshDesc), ctypes.POINTER(vp)]
+        L.qaf_mesh_destroy.argtypes = [vp]
+        L.qaf_mesh_sizes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+        L.qaf_mesh_tables.argtypes = [vp, vp, vp, vp, vp]
+        for n in ("qaf_fwd_trans", "qaf_bwd_trans", "qaf_xderiv", "qaf_yderiv", "qaf_laplacian"):
+            getattr(L, n).argtypes = [vp, vp, vp, vp]
+        L.qaf_symmetrize.argtypes = [vp, vp, vp]
+        L.qaf_dealias.argtypes = [vp, vp, vp]
+        L.qaf_vel.argtypes = [vp, vp, vp, vp, vp]
+        L.qaf_if_tables.argtypes = [vp, ctypes.POINTER(CParams), cp, vp, vp, vp]
+        L.qaf_integrate.argtypes = [vp, cp, cp, vp, vp, vp, vp, vp, vp, ctypes.c_double, vp]
+        L.qaf_nonlinear.argtypes = [vp, ctypes.POINTER(CParams), vp, vp, vp, vp, vp, vp, vp]
+        L.qaf_nonlinear_dbg.argtypes = [vp, ctypes.POINTER(CParams), vp, vp, vp, vp, vp, vp, vp, vp]
+        L.qaf_step.argtypes = [vp, ctypes.POINTER(CParams), cp, vp, vp, vp, cp, vp]
+        L.qaf_step_host.argtypes = [vp, ctypes.POINTER(CParams), cp, vp, vp, vp, cp]
+        L.qaf_last_diagnostics.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.qaf_check_finite.argtypes = [vp, vp]
+        L.qaf_diagnostics.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double), cp, vp]
+        L.qaf_state_load.argtypes = [vp, vp, vp, vp, vp]
+        L.qaf_state_store.argtypes = [vp, vp, vp, vp, vp]
+        L.qaf_state_advance.argtypes = [vp, ctypes.POINTER(CParams), cp, cp, vp]
+        L.qaf_state_advance_timed.argtypes = [vp, ctypes.POINTER(CParams), cp, cp, ctypes.POINTER(ctypes.c_double), vp]
+        L.qaf_launch_count.argtypes = [vp]
+        L.qaf_launch_count.restype = ctypes.c_uint64
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != OK:
+        msg = lib().qaf_last_error().decode(errors="replace")
+        if status == ERR_NONFINITE:
+            raise NonFiniteError(status, msg)
+        raise QafError(status, msg)
+
+
+def version() -> str:
+    return lib().qaf_version().decode()
+
+
+def supported(n: int, dtype: int = F32) -> bool:
+    return bool(lib().qaf_supported(n, dtype))
+
+
+def _stream():
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    import torch
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Mesh:
+    """Grid geometry, wave numbers, 2/3 mask and scratch (Basic/Mesh.cuh:48-113).
+
+    Fields are torch CUDA tensors: physical (ny, nx) real, spectral
+    (ny, nx//2+1) complex, in the reference's index order (x fastest).
+    """
+
+    def __init__(self, nx: int, ny: Optional[int] = None, lx: float = 2 * math.pi, ly: Optional[float] = None,
+                 dtype: int = F64):
+        self.nx, self.ny = nx, ny or nx
+        self.lx, self.ly = lx, ly or lx
+        self.dtype = dtype
+        self.nxh = nx // 2 + 1
+        h = ctypes.c_void_p()
+        _check(lib().qaf_mesh_create(ctypes.byref(MeshDesc(self.nx, self.ny, self.lx, self.ly, dtype)), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.qaf_mesh_destroy(h)
+            self._h = None
+
+    # -- tensors --------------------------------------------------------
+    @property
+    def real_dtype(self):
+        import torch
+        return torch.float64 if self.dtype == F64 else torch.float32
+
+    @property
+    def complex_dtype(self):
+        import torch
+        return torch.complex128 if self.dtype == F64 else torch.complex64
+
+    def new_spec(self):
+        import torch
+        return torch.zeros((self.ny, self.nxh), dtype=self.complex_dtype, device="cuda")
+
+    def new_phys(self):
+        import torch
+        return torch.zeros((self.ny, self.nx), dtype=self.real_dtype, device="cuda")
+
+    def _chk_spec(self, t):
+        if tuple(t.shape) != (self.ny, self.nxh) or t.dtype != self.complex_dtype:
+            raise ValueError(f"spectrum must be {(self.ny, self.nxh)} {self.complex_dtype}, got {tuple(t.shape)} {t.dtype}")
+        return _ptr(t)
+
+    def _chk_phys(self, t):
+        if tuple(t.shape) != (self.ny, self.nx) or t.dtype != self.real_dtype:
+            raise ValueError(f"physical field must be {(self.ny, self.nx)} {self.real_dtype}, got {tuple(t.shape)} {t.dtype}")
+        return _ptr(t)
+
+    def tables(self):
+        """kx, ky, k^2, cutoff as numpy arrays (waveinit / cutoff_func, Mesh.cuh:6-46)."""
+        import numpy as np
+        dt = np.float64 if self.dtype == F64 else np.float32
+        arrs = [np.empty((self.ny, self.nxh), dt) for _ in range(4)]
+        _check(lib().qaf_mesh_tables(self._h, *[a.ctypes.data_as(ctypes.c_void_p) for a in arrs]))
+        return arrs
+
+    # -- transforms and operators ---------------------------------------
+    def fwd_trans(self, phys, spec=None):
+        spec = self.new_spec() if spec is None else spec
+        _check(lib().qaf_fwd_trans(self._h, self._chk_phys(phys), self._chk_spec(spec), _stream()))
+        return spec
+
+    def bwd_trans(self, spec, phys=None):
+        phys = self.new_phys() if phys is None else phys
+        _check(lib().qaf_bwd_trans(self._h, self._chk_spec(spec), self._chk_phys(phys), _stream()))
+        return phys
+
+    def symmetrize(self, spec):
+        _check(lib().qaf_symmetrize(self._h, self._chk_spec(spec), _stream()))
+        return spec
+
+    def _unary(self, name, x, out):
+        out = self.new_spec() if out is None else out
+        _check(getattr(lib(), name)(self._h, self._chk_spec(x), self._chk_spec(out), _stream()))
+        return out
+
+    def xderiv(self, x, out=None):
+        return self._unary("qaf_xderiv", x, out)
+
+    def yderiv(self, x, out=None):
+        return self._unary("qaf_yderiv", x, out)
+
+    def laplacian(self, x, out=None):
+        return self._unary("qaf_laplacian", x, out)
+
+    def vel(self, w):
+        u, v = self.new_spec(), self.new_spec()
+        _check(lib().qaf_vel(self._h, self._chk_spec(w), self._chk_spec(u), self._chk_spec(v), _stream()))
+        return u, v
+
+    def dealias(self, x):
+        _check(lib().qaf_dealias(self._h, self._chk_spec(x), _stream()))
+        return x
+
+    def if_tables(self, p: Params, which: int):
+        import torch
+        IF = torch.empty((self.ny, self.nxh), dtype=self.real_dtype, device="cuda")
+        IFh = torch.empty_like(IF)
+        cp = p.c()
+        _check(lib().qaf_if_tables(self._h, ctypes.byref(cp), which, _ptr(IF), _ptr(IFh), _stream()))
+        return IF, IFh
+
+    def integrate(self, integ, stage, old, curr, new, nonl, IF, IFh, dt):
+        nl = None if nonl is None else self._chk_spec(nonl)
+        cu = None if curr is None else self._chk_spec(curr)
+        _check(lib().qaf_integrate(self._h, integ, stage, self._chk_spec(old), cu, self._chk_spec(new), nl,
+                                   _ptr(IF), _ptr(IFh), dt, _stream()))
+
+    # -- hot path -------------------------------------------------------
+    def nonlinear(self, p: Params, w, r1, r2, want_phys=False):
+        """N_w, N_r1, N_r2 at the given spectra; with want_phys also the row
+        pass's physical fields (w r1 r2 u v du/dx du/dy+dv/dx Lap r1 Lap r2 S p11 p12 p21)."""
+        import torch
+        outs = [self.new_spec() for _ in range(3)]
+        cp = p.c()
+        if want_phys:
+            phys = torch.zeros((13, self.ny, self.nx), dtype=self.real_dtype, device="cuda")
+            _check(lib().qaf_nonlinear_dbg(self._h, ctypes.byref(cp), self._chk_spec(w), self._chk_spec(r1),
+                                           self._chk_spec(r2), *[self._chk_spec(o) for o in outs], _ptr(phys),
+                                           _stream()))
+            return (*outs, phys)
+        _check(lib().qaf_nonlinear(self._h, ctypes.byref(cp), self._chk_spec(w), self._chk_spec(r1),
+                                   self._chk_spec(r2), *[self._chk_spec(o) for o in outs], _stream()))
+        return tuple(outs)
+
+    def step(self, p: Params, w, r1, r2, nsteps: int = 1, integrator: int = IFRK4):
+        """Advance the spectral state (w, r1, r2) in place by nsteps steps."""
+        cp = p.c()
+        _check(lib().qaf_step(self._h, ctypes.byref(cp), integrator, self._chk_spec(w), self._chk_spec(r1),
+                              self._chk_spec(r2), nsteps, _stream()))
+        return w, r1, r2
+
+    # -- resident state (load once, advance, store snapshots) -----------
+    def load(self, w, r1, r2):
+        _check(lib().qaf_state_load(self._h, self._chk_spec(w), self._chk_spec(r1), self._chk_spec(r2), _stream()))
+
+    def store(self, w=None, r1=None, r2=None):
+        w = self.new_spec() if w is None else w
+        r1 = self.new_spec() if r1 is None else r1
+        r2 = self.new_spec() if r2 is None else r2
+        _check(lib().qaf_state_store(self._h, self._chk_spec(w), self._chk_spec(r1), self._chk_spec(r2), _stream()))
+        return w, r1, r2
+
+    def advance(self, p: Params, nsteps: int = 1, integrator: int = IFRK4):
+        cp = p.c()
+        _check(lib().qaf_state_advance(self._h, ctypes.byref(cp), integrator, nsteps, _stream()))
+
+    def advance_timed(self, p: Params, nsteps: int = 1, integrator: int = IFRK4):
+        """Advance with CUDA events around each kernel: (row_ms, col_ms, launches)."""
+        cp = p.c()
+        out = (ctypes.c_double * 3)()
+        _check(lib().qaf_state_advance_timed(self._h, ctypes.byref(cp), integrator, nsteps, out, _stream()))
+        return out[0], out[1], int(out[2])
+
+    def launch_count(self) -> int:
+        return int(lib().qaf_launch_count(self._h))
+
+    def last_diagnostics(self):
+        """(energy, enstrophy) of the state left by the last step()."""
+        out = (ctypes.c_double * 2)()
+        _check(lib().qaf_last_diagnostics(self._h, out))
+        return out[0], out[1]
+
+    def check_finite(self):
+        _check(lib().qaf_check_finite(self._h, _stream()))
+
+    def diagnostics(self, w, nshells: int = 0):
+        """(energy, enstrophy, spectrum[nshells]) of a vorticity spectrum."""
+        import numpy as np
+        e, z = ctypes.c_double(), ctypes.c_double()
+        spec = np.zeros(max(nshells, 1))
+        _check(lib().qaf_diagnostics(self._h, self._chk_spec(w), ctypes.byref(e), ctypes.byref(z),
+                                     spec.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nshells, _stream()))
+        return e.value, z.value, (spec[:nshells] if nshells else None)

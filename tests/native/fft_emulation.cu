@@ -1,0 +1,81 @@
+// Host-side emulation of the team FFT in qaf_fft.cuh: every thread of a team
+// is run in a loop between the exchange phases, exactly as the kernels
+// interleave them with barriers; the result is compared with a direct DFT.
+// Built and run by tests/test_native_cpu.py (no GPU needed).
+#include "../../nature-control_b200/csrc/qaf_fft.cuh"
+#include <cmath>
+#include <cstdio>
+#include <vector>
+#include <complex>
+
+using namespace qaf;
+
+template <typename real, int L, int E, bool INV, int TWN, int P>
+void emulate_pass(std::vector<cplx<real>>& regs, const cplx<real>* tw) {
+    using Sc = Sched<L, E>;
+    constexpr int R = Sc::radix(P), S = Sc::span(P), TEAM = L / E;
+    for (int t = 0; t < TEAM; ++t) stockham_pass<real, L, E, R, S, INV, TWN>(t, &regs[t * E], tw);
+    if constexpr (P + 1 < Sc::passes) {
+        std::vector<cplx<real>> buf(L);
+        std::vector<int> hit(L, 0);
+        for (int t = 0; t < TEAM; ++t)
+            for (int slot = 0; slot < E; ++slot) {
+                int d = stockham_dest<L, E, R, S>(t, slot);
+                buf[d] = regs[t * E + slot];
+                hit[d]++;
+            }
+        for (int i = 0; i < L; ++i) if (hit[i] != 1) { std::printf("dest map not a permutation\n"); std::exit(1); }
+        for (int t = 0; t < TEAM; ++t)
+            for (int e = 0; e < E; ++e) regs[t * E + e] = buf[t + TEAM * e];
+        emulate_pass<real, L, E, INV, TWN, P + 1>(regs, tw);
+    }
+}
+
+template <typename real, int L, int E, bool INV>
+double check() {
+    constexpr int TWN = 2 * L, TEAM = L / E;
+    std::vector<cplx<real>> tw(TWN);
+    for (int m = 0; m < TWN; ++m) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * m / TWN;
+        tw[m] = mk<real>((real)cosl(a), (real)sinl(a));
+    }
+    std::vector<std::complex<double>> x(L);
+    unsigned s = 12345u + L * 7 + E;
+    for (int i = 0; i < L; ++i) {
+        s = s * 1664525u + 1013904223u; double a = (s >> 8) / 16777216.0 - 0.5;
+        s = s * 1664525u + 1013904223u; double b = (s >> 8) / 16777216.0 - 0.5;
+        x[i] = {a, b};
+    }
+    std::vector<cplx<real>> regs(L);
+    for (int t = 0; t < TEAM; ++t)
+        for (int e = 0; e < E; ++e) regs[t * E + e] = mk<real>((real)x[t + TEAM * e].real(), (real)x[t + TEAM * e].imag());
+    emulate_pass<real, L, E, INV, TWN, 0>(regs, tw.data());
+    double err = 0, ref = 0;
+    for (int k = 0; k < L; ++k) {
+        std::complex<long double> acc = 0;
+        for (int j = 0; j < L; ++j) {
+            long double a = (INV ? 2.0L : -2.0L) * 3.14159265358979323846264338327950288L * ((long long)j * k % L) / L;
+            acc += std::complex<long double>(x[j].real(), x[j].imag()) * std::complex<long double>(cosl(a), sinl(a));
+        }
+        int t = k % TEAM, e = k / TEAM;
+        cplx<real> g = regs[t * E + e];
+        double dr = (double)g.x - (double)acc.real(), di = (double)g.y - (double)acc.imag();
+        err += dr * dr + di * di; ref += (double)(acc.real() * acc.real() + acc.imag() * acc.imag());
+    }
+    return std::sqrt(err / ref);
+}
+
+#define CASE(real, L, E, INV, TOL) do { double e = check<real, L, E, INV>(); \
+    std::printf("%-6s L=%-5d E=%-3d inv=%d rel=%.3e\n", #real, L, E, (int)INV, e); if (!(e < TOL)) bad++; } while (0)
+
+int main() {
+    int bad = 0;
+    CASE(double, 8, 8, false, 1e-14);  CASE(double, 16, 8, true, 1e-14);
+    CASE(double, 32, 8, false, 1e-14); CASE(double, 64, 8, true, 1e-14);
+    CASE(double, 128, 4, false, 1e-14); CASE(double, 256, 16, true, 1e-14);
+    CASE(double, 512, 8, false, 1e-14); CASE(double, 1024, 8, true, 1e-14);
+    CASE(double, 1024, 16, false, 1e-14); CASE(double, 2048, 8, false, 1e-14);
+    CASE(float, 64, 8, false, 1e-6); CASE(float, 512, 8, true, 1e-6); CASE(float, 1024, 4, false, 1e-6);
+    std::printf(bad ? "FAIL\n" : "PASS\n");
+    return bad ? 1 : 0;
+}

@@ -1,0 +1,341 @@
+"""GPU parity tests: the CUDA path (through the C ABI) against the FP64 host
+oracle and against the golden vectors of the reference's own CUDA build.
+
+Tolerances: FP64 paths are compared by relative L2 norm at 1e-12 per call
+(a few ulps times log N of FFT rounding), 1e-10 after 1000 steps (the stated
+parity bar); FP32 paths at 1e-5 per call and 1e-4 after 100 steps."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+import qaf
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+L16 = 16 * np.pi
+SIZES = [16, 32, 64, 128, 256, 512, 1024]
+
+
+def dev(a, mesh):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype=mesh.complex_dtype)
+
+
+def devr(a, mesh):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype=mesh.real_dtype)
+
+
+def host(t):
+    a = t.detach().cpu().numpy()
+    return a.astype(np.complex128) if np.iscomplexobj(a) else a.astype(np.float64)
+
+
+def tol(mesh, f64, f32):
+    return f64 if mesh.dtype == qaf.F64 else f32
+
+
+def random_spec(n, seed, hermitian=False):
+    rng = np.random.default_rng(seed)
+    if hermitian:
+        return O.fwd(rng.standard_normal((n, n)))
+    return rng.standard_normal((n, n // 2 + 1)) + 1j * rng.standard_normal((n, n // 2 + 1))
+
+
+@pytest.mark.parametrize("dtype", [qaf.F64, qaf.F32])
+@pytest.mark.parametrize("n", SIZES)
+def test_transforms_against_oracle(cuda, n, dtype):
+    m = qaf.Mesh(n, lx=L16, dtype=dtype)
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((n, n))
+    X = host(m.fwd_trans(devr(x, m)))
+    assert O.rel_l2(X, O.fwd(x)) < tol(m, 1e-14, 1e-6)
+    # a non-Hermitian input: only the Hermitian part of kx = 0, n/2 counts
+    S = random_spec(n, n + 1)
+    y = host(m.bwd_trans(dev(S, m)))
+    assert O.rel_l2(y, O.bwd(S)) < tol(m, 1e-14, 1e-6)
+    # round trip
+    assert O.rel_l2(host(m.bwd_trans(m.fwd_trans(devr(x, m)))), x) < tol(m, 1e-14, 1e-6)
+
+
+@pytest.mark.parametrize("dtype", [qaf.F64, qaf.F32])
+def test_spectral_operators_against_oracle(cuda, dtype):
+    n = 64
+    m = qaf.Mesh(n, lx=L16, dtype=dtype)
+    p = O.params(n=n)
+    S = random_spec(n, 7)
+    t = tol(m, 1e-15, 1e-6)
+    assert O.rel_l2(host(m.xderiv(dev(S, m))), O.xderiv(p, S)) < t
+    assert O.rel_l2(host(m.yderiv(dev(S, m))), O.yderiv(p, S)) < t
+    assert O.rel_l2(host(m.laplacian(dev(S, m))), O.laplacian(p, S)) < t
+    u, v = m.vel(dev(S, m))
+    ou, ov = O.vel(p, S)
+    assert O.rel_l2(host(u), ou) < t and O.rel_l2(host(v), ov) < t
+    assert O.rel_l2(host(m.dealias(dev(S, m))), O.dealias(p, S)) < t
+    sym = dev(S, m)
+    m.symmetrize(sym)
+    ref = S.copy()
+    phys = np.empty((n, n))
+    O.lib().oracle_bwd_mutating(n, n, O._p(ref), O._p(phys))
+    assert O.rel_l2(host(sym), ref) < t
+    kx, ky, k2, cut = m.tables()
+    okx, oky, ok2, ocut = O.tables(p)
+    assert np.allclose(kx, okx) and np.allclose(ky, oky) and np.allclose(k2, ok2) and np.array_equal(cut, ocut)
+
+
+@pytest.mark.parametrize("dtype", [qaf.F64, qaf.F32])
+@pytest.mark.parametrize("integ,stages", [(qaf.IFRK4, 5), (qaf.IFRK2, 3), (qaf.IFE, 1)])
+def test_if_tables_and_stage_kernels(cuda, dtype, integ, stages):
+    # wlin_func / r1lin_func and integrate_funcXD applied stage by stage, against numpy
+    n = 32
+    m = qaf.Mesh(n, lx=L16, dtype=dtype)
+    p = O.params(n=n, re=0.7, rf=0.2, dt=0.01)
+    qp = qaf.Params(re=0.7, rf=0.2, dt=0.01)
+    for which in (0, 1):
+        IF, IFh = m.if_tables(qp, which)
+        oIF, oIFh = O.if_tables(p, which, 0.01)
+        assert np.allclose(host(IF), oIF, rtol=tol(m, 1e-15, 1e-6)) and np.allclose(host(IFh), oIFh, rtol=tol(m, 1e-15, 1e-6))
+    IF, IFh = m.if_tables(qp, 0)
+    oIF, oIFh = host(IF), host(IFh)
+    old, nl = random_spec(n, 1), random_spec(n, 2)
+    curr, new = m.new_spec(), m.new_spec()
+    dt = 0.01
+    c_ref, n_ref = np.zeros_like(old), np.zeros_like(old)
+    first = 1 if integ == qaf.IFE else 0
+    for s in range(first, stages + first if integ == qaf.IFE else stages):
+        m.integrate(integ, s, dev(old, m), curr, new, dev(nl, m), IF, IFh, dt)
+        an = nl * dt
+        if integ == qaf.IFRK4:
+            if s == 0: n_ref, c_ref = old * oIF, old.copy()
+            elif s == 1: n_ref, c_ref = n_ref + 1 / 6 * oIF * an, (old + an / 2) * oIFh
+            elif s == 2: n_ref, c_ref = n_ref + 1 / 3 * oIFh * an, old * oIFh + an / 2
+            elif s == 3: n_ref, c_ref = n_ref + 1 / 3 * oIFh * an, old * oIF + an * oIFh
+            else: n_ref = n_ref + an / 6
+        elif integ == qaf.IFRK2:
+            if s == 0: n_ref, c_ref = old * oIF, old.copy()
+            elif s == 1: n_ref, c_ref = n_ref + 0.5 * oIF * an, (old + an) * oIFh
+            else: n_ref = n_ref + 0.5 * an
+        else:
+            n_ref = (old + an) * oIF
+        t = tol(m, 1e-14, 1e-5)
+        assert O.rel_l2(host(new), n_ref) < t
+        if integ != qaf.IFE:
+            assert O.rel_l2(host(curr), c_ref) < t
+
+
+@pytest.mark.parametrize("dtype", [qaf.F64, qaf.F32])
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512])
+def test_nonlinear_against_oracle(cuda, n, dtype):
+    # full-spectrum input with non-Hermitian kx = 0 and kx = n/2 columns, as in RK stages 2-4
+    m = qaf.Mesh(n, lx=L16, dtype=dtype)
+    p = O.params(n=n)
+    rng = np.random.default_rng(n + 11)
+    st = [random_spec(n, 100 + n + k) * 1e-3 * (n / 32) for k in range(3)]
+    st[0] *= 30
+    ow, o1, o2 = O.nonlinear(p, *st)
+    gw, g1, g2 = m.nonlinear(qaf.Params(), *[dev(a, m) for a in st])
+    t = tol(m, 2e-12, 2e-5)
+    for g, o in zip((gw, g1, g2), (ow, o1, o2)):
+        assert O.rel_l2(host(g), o) < t
+
+
+def test_nonlinear_physical_fields_against_oracle(cuda):
+    n = 32
+    m = qaf.Mesh(n, lx=L16, dtype=qaf.F64)
+    p = O.params(n=n)
+    st = [random_spec(n, 40 + k, hermitian=True) * 1e-3 for k in range(3)]
+    *_, oph = O.nonlinear(p, *st, want_phys=True)
+    *_, gph = m.nonlinear(qaf.Params(), *[dev(a, m) for a in st], want_phys=True)
+    gph = host(gph)
+    # oracle order: w r1 r2 u v S p11 p12 p21; library order: w r1 r2 u v ux sh Lr1 Lr2 S p11 p12 p21
+    for oi, gi in ((0, 0), (1, 1), (2, 2), (3, 3), (4, 4), (5, 9), (6, 10), (7, 11), (8, 12)):
+        assert O.rel_l2(gph[gi], oph[oi]) < 1e-13, (oi, gi)
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_nonlinear_against_reference_build(cuda, n):
+    g = golden(f"ref_nl_rand{n}.npz")
+    m = qaf.Mesh(n, lx=L16, dtype=qaf.F64)
+    out = m.nonlinear(qaf.Params(), dev(g["w"], m), dev(g["r1"], m), dev(g["r2"], m))
+    for a, key in zip(out, ("wn", "r1n", "r2n")):
+        assert O.rel_l2(host(a), g[key]) < 1e-13
+
+
+@pytest.mark.parametrize("k", range(5))
+def test_nonlinear_known_answers_gpu(cuda, k):
+    from golden.make_golden import kat_fields
+    n = 128
+    m = qaf.Mesh(n, lx=2 * np.pi, dtype=qaf.F64)
+    w, r1, r2, e0, e1, e2 = kat_fields(k)
+    qp = qaf.Params(re=0.1, er=0.1, alpha=0.2, lam=0.1, rf=0.000075)
+    nl = m.nonlinear(qp, *[m.fwd_trans(devr(a, m)) for a in (w, r1, r2)])
+    dev_ = [np.abs(host(m.bwd_trans(a)) - b).max() / np.abs(b).max() for a, b in zip(nl, (e0, e1, e2))]
+    assert dev_[0] < 2e-7 and dev_[1] < (2e-8 if k == 3 else 1e-12) and dev_[2] < 1e-12
+
+
+@pytest.mark.parametrize("integ", [qaf.IFRK4, qaf.IFRK2, qaf.IFE])
+@pytest.mark.parametrize("n", [16, 32, 64, 128])
+def test_steps_against_oracle_f64(cuda, n, integ):
+    m = qaf.Mesh(n, lx=L16, dtype=qaf.F64)
+    p = O.params(n=n)
+    s0 = O.initial_spectra(2, n)
+    ref = O.step(p, *s0, 5, integ)
+    st = [dev(a, m) for a in s0]
+    m.step(qaf.Params(), *st, nsteps=5, integrator=integ)
+    for g, o in zip(st, ref):
+        assert O.rel_l2(host(g), o) < 1e-13
+
+
+def test_rk4_matches_reference_build_32_and_64(cuda):
+    g = golden("ref_run32.npz")
+    m = qaf.Mesh(32, lx=L16, dtype=qaf.F64)
+    st = [dev(g[f"{k}_0"], m) for k in ("w", "r1", "r2")]
+    prev = 0
+    for s in (1, 2, 10, 20):
+        m.step(qaf.Params(), *st, nsteps=s - prev)
+        prev = s
+        for t, k in zip(st, ("w", "r1", "r2")):
+            assert O.rel_l2(host(t), g[f"{k}_{s}"]) < 1e-13, (s, k)
+    g = golden("ref_run64_s100.npz")
+    m = qaf.Mesh(64, lx=L16, dtype=qaf.F64)
+    st = [dev(a, m) for a in O.initial_spectra(0, 64)]
+    m.step(qaf.Params(), *st, nsteps=100)
+    for t, k in zip(st, ("w", "r1", "r2")):
+        assert O.rel_l2(host(t), g[k]) < 1e-12
+
+
+def test_f64_1000_steps_match_reference_build_128(cuda):
+    # the parity configuration: 128^2, L = 16 pi, FP64, IF-RK4, dt = 1e-3,
+    # 1000 steps, seed 0; bar: relative L2 <= 1e-10 against the reference's build
+    g = golden("ref_run128_s1000.npz")
+    m = qaf.Mesh(128, lx=L16, dtype=qaf.F64)
+    st = [dev(a, m) for a in O.initial_spectra(0, 128)]
+    m.load(*st)
+    m.advance(qaf.Params(), nsteps=1000)
+    m.store(*st)
+    for t, k in zip(st, ("w", "r1", "r2")):
+        assert O.rel_l2(host(t), g[k]) < 1e-10, k
+
+
+def test_f32_100_steps_against_oracle_128(cuda):
+    # FP32 path: relative L2 <= 1e-4 of the FP64 oracle after 100 steps
+    n = 128
+    m = qaf.Mesh(n, lx=L16, dtype=qaf.F32)
+    s0 = O.initial_spectra(0, n)
+    ref = O.step(O.params(n=n), *s0, 100)
+    st = [dev(a, m) for a in s0]
+    m.step(qaf.Params(), *st, nsteps=100)
+    for t, o in zip(st, ref):
+        assert O.rel_l2(host(t), o) < 1e-4
+
+
+@pytest.mark.parametrize("n", [256, 1024])
+def test_large_grid_one_step_against_oracle(cuda, n):
+    m = qaf.Mesh(n, lx=L16, dtype=qaf.F64)
+    p = O.params(n=n, dt=5e-4)
+    s0 = O.initial_spectra(1, n)
+    ref = O.step(p, *s0, 1)
+    st = [dev(a, m) for a in s0]
+    m.step(qaf.Params(dt=5e-4), *st, nsteps=1)
+    for t, o in zip(st, ref):
+        assert O.rel_l2(host(t), o) < 1e-12
+
+
+def test_alpha_field_and_variants_against_oracle(cuda):
+    n = 64
+    m = qaf.Mesh(n, lx=L16, dtype=qaf.F64)
+    x = np.arange(n) * L16 / n
+    X, Y = np.meshgrid(x, x)
+    alpha = 1.0 + 0.3 * np.sin(X / 4) * np.cos(Y / 8)
+    s0 = O.initial_spectra(6, n)
+    for advect in (1, 0):
+        p = O.params(n=n, rf=0.3, lam=0.2, advect_omega=advect)
+        ref = O.step(p, *s0, 4, alpha_field=alpha)
+        st = [dev(a, m) for a in s0]
+        m.step(qaf.Params(rf=0.3, lam=0.2, advect_omega=advect, alpha_field=devr(alpha, m)), *st, nsteps=4)
+        for t, o in zip(st, ref):
+            assert O.rel_l2(host(t), o) < 1e-13
+
+
+def test_taylor_green_decay_gpu(cuda):
+    for n, dtype, t in ((64, qaf.F64, 1e-13), (1024, qaf.F64, 1e-12), (1024, qaf.F32, 1e-6)):
+        m = qaf.Mesh(n, lx=2 * np.pi, dtype=dtype)
+        x = np.arange(n) * 2 * np.pi / n
+        X, Y = np.meshgrid(x, x)
+        w0 = -2 * np.cos(X) * np.cos(Y)
+        z = np.zeros_like(w0)
+        st = [m.fwd_trans(devr(a, m)) for a in (w0, z, z)]
+        m.step(qaf.Params(re=40, er=40, rf=0, alpha=0.2, dt=0.02), *st, nsteps=20)
+        wt = host(m.bwd_trans(st[0]))
+        assert np.abs(wt - w0 * np.exp(-2 * 20 * 0.02 / 40)).max() < t * 2
+
+
+def test_diagnostics_against_oracle(cuda):
+    n = 64
+    m = qaf.Mesh(n, lx=L16, dtype=qaf.F64)
+    p = O.params(n=n)
+    s0 = O.initial_spectra(3, n)
+    ref = O.step(p, *s0, 3)
+    st = [dev(a, m) for a in s0]
+    m.step(qaf.Params(), *st, nsteps=3)
+    torch.cuda.synchronize()
+    e, z = m.last_diagnostics()
+    oe, oz, ospec = O.diagnostics(p, ref[0], nshells=40)
+    assert np.isclose(e, oe, rtol=1e-10) and np.isclose(z, oz, rtol=1e-10)
+    ge, gz, gspec = m.diagnostics(st[0], nshells=40)
+    assert np.isclose(ge, oe, rtol=1e-10) and np.isclose(gz, oz, rtol=1e-10)
+    assert np.allclose(gspec, ospec, rtol=1e-10, atol=1e-30)
+
+
+def test_nonfinite_state_is_reported(cuda):
+    # failure detection without a GPU fault: a NaN planted in the host-side
+    # initial field propagates and the step reports it
+    n = 32
+    m = qaf.Mesh(n, lx=L16, dtype=qaf.F64)
+    s0 = [a.copy() for a in O.initial_spectra(0, n)]
+    s0[1][3, 2] = np.nan
+    st = [dev(a, m) for a in s0]
+    m.step(qaf.Params(), *st, nsteps=2)
+    with pytest.raises(qaf.NonFiniteError):
+        m.check_finite()
+    st = [dev(a, m) for a in O.initial_spectra(0, n)]
+    m.step(qaf.Params(), *st, nsteps=2)
+    m.check_finite()
+
+
+def test_resident_state_equals_step_and_host_step(cuda):
+    n = 64
+    m = qaf.Mesh(n, lx=L16, dtype=qaf.F32)
+    s0 = O.initial_spectra(8, n)
+    a = [dev(x, m) for x in s0]
+    m.step(qaf.Params(), *a, nsteps=6)
+    b = [dev(x, m) for x in s0]
+    m.load(*b)
+    m.advance(qaf.Params(), nsteps=2)
+    m.advance(qaf.Params(), nsteps=4)
+    m.store(*b)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    h = [np.ascontiguousarray(x.astype(np.complex64)) for x in s0]
+    cp = qaf.Params().c()
+    import ctypes
+    rc = qaf.lib().qaf_step_host(m._h, ctypes.byref(cp), qaf.IFRK4, *[ctypes.c_void_p(x.ctypes.data) for x in h], 6)
+    assert rc == 0
+    for x, y in zip(a, h):
+        assert np.array_equal(host(x).astype(np.complex64), y)
+
+
+def test_invalid_arguments_are_rejected(cuda):
+    m = qaf.Mesh(32, lx=L16, dtype=qaf.F64)
+    st = [m.new_spec() for _ in range(3)]
+    with pytest.raises(qaf.QafError):
+        m.step(qaf.Params(re=0.0), *st)
+    with pytest.raises(qaf.QafError):
+        m.step(qaf.Params(), *st, integrator=7)
+    with pytest.raises(ValueError):
+        m.step(qaf.Params(), st[0][:, :5].contiguous(), st[1], st[2])
+    m48 = qaf.Mesh(48, lx=L16, dtype=qaf.F64)
+    s48 = [m48.new_spec() for _ in range(3)]
+    with pytest.raises(qaf.QafError) as e:
+        m48.step(qaf.Params(), *s48)
+    assert e.value.status == qaf.ERR_UNSUPPORTED
