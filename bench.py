@@ -36,7 +36,6 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "nature-control_b200"))
-sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "grid-pt*steps/s at 1024^2, IF-RK4 (w, r1, r2)"
 UNIT = "grid-pt*steps/s"
@@ -146,16 +145,6 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(loaded)}
 
 
-def initial_state(mesh, seed):
-    """Seeded random-Q state (include/qaf_init.h), transformed by the library."""
-    import numpy as np
-    import torch
-
-    import oracle as O   # only for the numpy restatement of the seeded generator
-    w, r1, r2 = O.random_q_init(seed, mesh.nx)
-    return [mesh.fwd_trans(torch.from_numpy(a).to("cuda", dtype=mesh.real_dtype)) for a in (w, r1, r2)]
-
-
 def max_over_ranks(x, world):
     if world == 1:
         return x
@@ -177,6 +166,7 @@ def barrier(world):
 def cpu_baseline(n, steps, dtype_name):
     """The FP64 host oracle (a restatement of the reference's scheme) on the
     host cores, on a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     p = O.params(n=n, L=L, dt=DT)
     s0 = O.initial_spectra(SEED, n)
@@ -191,7 +181,6 @@ def cpu_baseline(n, steps, dtype_name):
 
 
 def run_qaf(a, world, rank, local):
-    import numpy as np
     import torch
 
     import qaf
@@ -200,7 +189,7 @@ def run_qaf(a, world, rank, local):
     n = a.n
     mesh = qaf.Mesh(n, lx=L, dtype=dtype)
     p = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=DT, q_lin=1.0, advect_omega=1)
-    state = initial_state(mesh, SEED)
+    state = mesh.random_q(SEED)
     mesh.load(*state)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")   # > 126 MB L2
 
@@ -244,8 +233,6 @@ def run_qaf(a, world, rank, local):
             traffic = None
 
     # ---- end to end through the public API, host I/O every step ----------
-    import oracle as O
-    x = np.arange(n) * L / n
     alpha_host = torch.ones((n, n), dtype=mesh.real_dtype).pin_memory()
     alpha_dev = torch.empty((n, n), dtype=mesh.real_dtype, device="cuda")
     pe = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=DT, alpha_field=alpha_dev)

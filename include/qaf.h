@@ -160,6 +160,14 @@ qaf_status qaf_state_advance_timed(qaf_mesh* mesh, const qaf_params* p, qaf_inte
 /* Number of kernels this mesh has launched so far. */
 uint64_t qaf_launch_count(const qaf_mesh* mesh);
 
+/* ---- seeded initial state -------------------------------------------------
+ * The reference reads its initial Q from CSV files or fills it with libc
+ * rand() (friction.cu:21-41, :164-185). Here: r1, r2 ~ U(lo, hi) from the
+ * SplitMix64 stream of include/qaf_init.h (r1 first, then r2, in physical order
+ * i + j*nx), w = 0, each transformed with FwdTrans into the given spectra. */
+qaf_status qaf_init_random_q(qaf_mesh* mesh, uint64_t seed, double lo, double hi, void* w, void* r1, void* r2,
+                             void* stream);
+
 /* ---- diagnostics of a spectral state (post_process/) --------------------- */
 /* energy and enstrophy as in qaf_last_diagnostics, and the shell spectrum
  * E(k_s), k_s = s dk, s < nshells, dk = 2 pi / Lx (EnergySpec.cu:81-96),

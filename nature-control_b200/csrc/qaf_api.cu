@@ -1,6 +1,7 @@
 // qaf_api.cu — the C ABI of include/qaf.h: meshes, workspaces, launch
 // configuration per grid size and precision, and the step driver.
 #include "qaf.h"
+#include "qaf_init.h"
 #include "qaf_kernels.cuh"
 #include "qaf_ops.cuh"
 
@@ -43,17 +44,31 @@ constexpr int kMinN = 16, kMaxN = 1024;
 template <typename real, int N>
 struct Cfg {
     static constexpr int H = N / 2;
-    static constexpr int W = (sizeof(real) == 4 ? 8 : 4) < H ? (sizeof(real) == 4 ? 8 : 4) : H;  // columns per CTA
-    static constexpr int EC = 8;                                                              // column FFT values/thread
-    static constexpr int ER = (sizeof(real) == 4 ? 8 : 4) < H ? (sizeof(real) == 4 ? 8 : 4) : H;  // row FFT values/thread
-    static constexpr int TEAM_R = H / ER;
-    static constexpr int ROWS = (TEAM_R >= 128) ? 1 : (128 / TEAM_R <= N ? 128 / TEAM_R : N);
+    static constexpr bool F32 = sizeof(real) == 4;
+    // CTAs per SM the register budget is sized for (FP64 kernels need > 128 registers)
+    static constexpr int MINB = F32 ? 2 : 1;
+    // column kernel: W kx-columns per CTA, EC values per thread of a length-N y-FFT
+    static constexpr int W = 4 < H ? 4 : H;
+    static constexpr int EC = 16 < N ? 16 : N;
     static constexpr int COL_THREADS = W * (N / EC);
-    static constexpr int ROW_THREADS = ROWS * TEAM_R;
     static constexpr size_t COL_SMEM = (size_t)(W * N + 2 * N) * sizeof(cplx<real>);
-    static constexpr size_t ROW_SMEM = (size_t)ROWS * H * sizeof(cplx<real>);
     static constexpr int COL_BLOCKS = 3 * (H / W) + 3;
+    // row kernel: ER values per thread of a length-N x-FFT, ROWS rows per CTA
+    static constexpr int ER = 8 < N ? 8 : N;
+    static constexpr int TEAM_R = N / ER;
+    static constexpr int ROWS_A = 256 / TEAM_R > 0 ? 256 / TEAM_R : 1;
+    static constexpr int ROWS_B = N / 8 > 0 ? N / 8 : 1;
+    static constexpr int ROWS = ROWS_A < ROWS_B ? ROWS_A : ROWS_B;
+    static constexpr int ROW_THREADS = ROWS * TEAM_R;
+    static constexpr size_t ROW_SMEM = RowKernel<real, N, ER, ROWS>::SMEM;
     static constexpr int ROW_BLOCKS = N / ROWS;
+    // standalone transforms: half-length row FFTs
+    static constexpr int ERT = (F32 ? 8 : 4) < H ? (F32 ? 8 : 4) : H;
+    static constexpr int TEAM_T = H / ERT;
+    static constexpr int ROWS_T = (TEAM_T >= 128) ? 1 : (128 / TEAM_T <= N ? 128 / TEAM_T : N);
+    static constexpr int ROWT_THREADS = ROWS_T * TEAM_T;
+    static constexpr size_t ROWT_SMEM = (size_t)ROWS_T * H * sizeof(cplx<real>);
+    static constexpr int ROWT_BLOCKS = N / ROWS_T;
 };
 
 template <typename real>
@@ -209,25 +224,25 @@ struct Launch {
     static qaf_status setup() {
         static bool done = false;
         if (done) return QAF_OK;
-        QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
-        QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::ROW_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::W, C::EC, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::ROW_SMEM));
         QAF_CUDA(cudaFuncSetAttribute(col_ifft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
         QAF_CUDA(cudaFuncSetAttribute(col_fft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
         done = true;
         return QAF_OK;
     }
     static void col(const StageArgs<real>& a, cudaStream_t st) {
-        col_kernel<real, N, C::W, C::EC><<<C::COL_BLOCKS, C::COL_THREADS, C::COL_SMEM, st>>>(a);
+        col_kernel<real, N, C::W, C::EC, C::MINB><<<C::COL_BLOCKS, C::COL_THREADS, C::COL_SMEM, st>>>(a);
     }
     static void row(const StageArgs<real>& a, cudaStream_t st) {
-        row_kernel<real, N, C::ER, C::ROWS><<<C::ROW_BLOCKS, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
+        row_kernel<real, N, C::ER, C::ROWS, C::MINB><<<C::ROW_BLOCKS, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
     }
     static void bwd(const cplx<real>* spec, cplx<real>* T, real* phys, const cplx<real>* tw, cudaStream_t st) {
         col_ifft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COL_THREADS, C::COL_SMEM, st>>>(spec, T, tw);
-        row_c2r_kernel<real, N, C::ER, C::ROWS><<<C::ROW_BLOCKS, C::ROW_THREADS, C::ROW_SMEM, st>>>(T, phys, tw);
+        row_c2r_kernel<real, N, C::ERT, C::ROWS_T><<<C::ROWT_BLOCKS, C::ROWT_THREADS, C::ROWT_SMEM, st>>>(T, phys, tw);
     }
     static void fwd(const real* phys, cplx<real>* T, cplx<real>* spec, const cplx<real>* tw, cudaStream_t st) {
-        row_r2c_kernel<real, N, C::ER, C::ROWS><<<C::ROW_BLOCKS, C::ROW_THREADS, C::ROW_SMEM, st>>>(phys, T, tw);
+        row_r2c_kernel<real, N, C::ERT, C::ROWS_T><<<C::ROWT_BLOCKS, C::ROWT_THREADS, C::ROWT_SMEM, st>>>(phys, T, tw);
         col_fft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COL_THREADS, C::COL_SMEM, st>>>(T, spec, tw);
     }
 };
@@ -766,6 +781,36 @@ qaf_status qaf_diagnostics(qaf_mesh* m, const void* w, double* energy, double* e
     if (!w) return fail(QAF_ERR_INVALID, "null pointer");
     if (m->desc.dtype == QAF_F64) return diag_impl<double>(m, w, energy, enstrophy, spectrum, nshells, (cudaStream_t)stream);
     return diag_impl<float>(m, w, energy, enstrophy, spectrum, nshells, (cudaStream_t)stream);
+}
+
+qaf_status qaf_init_random_q(qaf_mesh* m, uint64_t seed, double lo, double hi, void* w, void* r1, void* r2,
+                             void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!w || !r1 || !r2) return fail(QAF_ERR_INVALID, "null pointer");
+    if (!(hi >= lo)) return fail(QAF_ERR_INVALID, "need lo <= hi");
+    const size_t np = phys_elems(m);
+    std::vector<double> hw(np), h1(np), h2(np);
+    qaf_random_q_init(seed, m->desc.nx, m->desc.ny, lo, hi, hw.data(), h1.data(), h2.data());
+    const size_t rb = real_bytes(m);
+    void* d = nullptr;
+    QAF_CUDA(cudaMalloc(&d, np * rb));
+    void* out[3] = {w, r1, r2};
+    const std::vector<double>* src[3] = {&hw, &h1, &h2};
+    qaf_status st = QAF_OK;
+    std::vector<float> tmp;
+    for (int f = 0; f < 3 && st == QAF_OK; ++f) {
+        const void* hp = src[f]->data();
+        if (rb == 4) { tmp.assign(src[f]->begin(), src[f]->end()); hp = tmp.data(); }
+        cudaError_t e = cudaMemcpy(d, hp, np * rb, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { st = fail(QAF_ERR_CUDA, std::string("qaf_init_random_q: ") + cudaGetErrorString(e)); break; }
+        st = qaf_fwd_trans(m, d, out[f], stream);
+        if (st == QAF_OK) {
+            e = cudaStreamSynchronize((cudaStream_t)stream);
+            if (e != cudaSuccess) st = fail(QAF_ERR_CUDA, std::string("qaf_init_random_q: ") + cudaGetErrorString(e));
+        }
+    }
+    cudaFree(d);
+    return st;
 }
 
 }  // extern "C"

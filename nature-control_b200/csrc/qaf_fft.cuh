@@ -51,7 +51,13 @@ QAF_HD double cos16(int k) {
 QAF_HD double sin16(int k) { return cos16(k + 12); }   // sin(x) = cos(x - pi/2)
 
 QAF_HDC int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
-QAF_HDC int bitrev(int x, int bits) { return bits == 0 ? 0 : ((x & 1) << (bits - 1)) | bitrev(x >> 1, bits - 1); }
+// iterative (not recursive) so that, with constant arguments after unrolling,
+// the device compiler folds it and register arrays indexed by it stay in registers
+QAF_HDC int bitrev(int x, int bits) {
+    int r = 0;
+    for (int i = 0; i < bits; ++i) { r = (r << 1) | (x & 1); x >>= 1; }
+    return r;
+}
 
 // In-register DFT of R = 2, 4, 8 or 16 points: y[r] = sum_q x[q] W_R^{qr},
 // W_R = exp(-2 pi i / R) (forward) or exp(+2 pi i / R) (INV). Iterative
@@ -88,36 +94,6 @@ QAF_HD void small_dft(cplx<real>* x) {
     for (int q = 0; q < R; ++q) x[q] = y[q];
 }
 
-// One Stockham pass of radix R on span S (the product of the radices already
-// applied) for a length-L transform, E values per thread. Butterfly
-// b = t + TEAM*s (s < E/R) reads elements b + q*L/R, i.e. register s + q*(E/R),
-// applies W_{S R}^{q k} (k = b mod S), and leaves output r in register
-// s + r*(E/R). tw[m] = exp(-2 pi i m / TWN) with TWN a multiple of L.
-template <typename real, int L, int E, int R, int S, bool INV, int TWN>
-QAF_HD void stockham_pass(int t, cplx<real>* v, const cplx<real>* tw) {
-    constexpr int TEAM = L / E;
-    constexpr int NB = E / R;
-    static_assert(E % R == 0 && L % (S * R) == 0, "pass shape");
-#pragma unroll
-    for (int s = 0; s < NB; ++s) {
-        cplx<real> x[R];
-        const int b = t + TEAM * s;
-        const int k = b % S;
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-            x[q] = v[s + q * NB];
-            if (S > 1 && q > 0) {
-                // W_{S R}^{q k} = W_TWN^{q k TWN/(S R)}, q k < S R
-                const int m = q * k * (TWN / (S * R));
-                x[q] = ctw<INV>(x[q], tw[m]);
-            }
-        }
-        small_dft<real, R, INV>(x);
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[s + r * NB] = x[r];
-    }
-}
-
 // Where register slot (s + r*NB) of thread t lands after the pass above.
 template <int L, int E, int R, int S>
 QAF_HD int stockham_dest(int t, int slot) {
@@ -143,32 +119,93 @@ struct Sched {
     }
 };
 
-// Team FFT driver. `xchg` provides the team's shared buffer:
-//   xchg.write(index, value), xchg.sync(), xchg.read(index) -> value.
-// Between passes every thread writes its E values to their destinations,
-// the team synchronises, reads back its own E strided elements and
-// synchronises again (so the buffer can be reused by the next exchange).
-template <typename real, int L, int E, bool INV, int TWN, int P, class X>
-QAF_HD void team_pass(int t, cplx<real>* v, const cplx<real>* tw, X& xchg) {
+// Team FFT with per-thread twiddle bases. In pass P (span S, radix R) the
+// butterfly b = t + TEAM*s needs W_{S R}^{q k}, q < R, k = b mod S. The base
+// W_{S R}^{k} depends only on (t, P, s), not on the data, so a team computes
+// its bases once (init) and every transform then forms the powers by complex
+// multiplication — no twiddle loads inside a transform. The powers carry a
+// rounding error of about q ulps (q < 16).
+template <int L, int E>
+struct TwLayout {
     using Sc = Sched<L, E>;
-    constexpr int R = Sc::radix(P);
-    constexpr int S = Sc::span(P);
-    stockham_pass<real, L, E, R, S, INV, TWN>(t, v, tw);
-    if constexpr (P + 1 < Sc::passes) {
-        constexpr int TEAM = L / E;
+    QAF_HD static constexpr int offset(int P) {   // first base of pass P (P >= 1)
+        int o = 0;
+        for (int p = 1; p < P; ++p) o += E / Sc::radix(p);
+        return o;
+    }
+    static constexpr int count = Sc::passes > 1 ? offset(Sc::passes) : 0;
+};
+
+template <typename real, int L, int E, bool INV, int P>
+QAF_HD void stockham_pass_tw(int t, cplx<real>* v, const cplx<real>* base) {
+    using Sc = Sched<L, E>;
+    constexpr int R = Sc::radix(P), NB = E / R;
 #pragma unroll
-        for (int slot = 0; slot < E; ++slot) xchg.write(stockham_dest<L, E, R, S>(t, slot), v[slot]);
-        xchg.sync();
+    for (int s = 0; s < NB; ++s) {
+        cplx<real> x[R];
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = xchg.read(t + TEAM * e);
-        xchg.sync();
-        team_pass<real, L, E, INV, TWN, P + 1, X>(t, v, tw, xchg);
+        for (int q = 0; q < R; ++q) x[q] = v[s + q * NB];
+        if constexpr (P > 0) {
+            cplx<real> w = base[TwLayout<L, E>::offset(P) + s];
+            if (INV) w.y = -w.y;
+            cplx<real> wq = w;
+#pragma unroll
+            for (int q = 1; q < R; ++q) {
+                x[q] = cmul(x[q], wq);
+                if (q + 1 < R) wq = cmul(wq, w);
+            }
+        }
+        small_dft<real, R, INV>(x);
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[s + r * NB] = x[r];
     }
 }
 
-template <typename real, int L, int E, bool INV, int TWN, class X>
-QAF_HD void team_fft(int t, cplx<real>* v, const cplx<real>* tw, X& xchg) {
-    team_pass<real, L, E, INV, TWN, 0, X>(t, v, tw, xchg);
-}
+template <typename real, int L, int E>
+struct TeamFFT {
+    using Sc = Sched<L, E>;
+    static constexpr int TEAM = L / E;
+    static constexpr int NBASE = TwLayout<L, E>::count;
+    cplx<real> base[NBASE > 0 ? NBASE : 1];
+
+    // tw[m] = exp(-2 pi i m / TWN), TWN a multiple of L
+    template <int TWN>
+    QAF_HD void init(int t, const cplx<real>* tw) {
+        init_pass<TWN, 1>(t, tw);
+    }
+    template <int TWN, int P>
+    QAF_HD void init_pass(int t, const cplx<real>* tw) {
+        if constexpr (P < Sc::passes) {
+            constexpr int R = Sc::radix(P), S = Sc::span(P), NB = E / R;
+#pragma unroll
+            for (int s = 0; s < NB; ++s) {
+                const int k = (t + TEAM * s) % S;
+                base[TwLayout<L, E>::offset(P) + s] = tw[k * (TWN / (S * R))];
+            }
+            init_pass<TWN, P + 1>(t, tw);
+        }
+    }
+
+    // In-place transform of v (distribution: thread t holds element t + TEAM*e).
+    // `xchg` is the team's shared buffer: write(index, value), sync(), read(index).
+    template <bool INV, class X>
+    QAF_HD void run(int t, cplx<real>* v, X& xchg) const {
+        pass<INV, 0, X>(t, v, xchg);
+    }
+    template <bool INV, int P, class X>
+    QAF_HD void pass(int t, cplx<real>* v, X& xchg) const {
+        constexpr int R = Sc::radix(P), S = Sc::span(P);
+        stockham_pass_tw<real, L, E, INV, P>(t, v, base);
+        if constexpr (P + 1 < Sc::passes) {
+#pragma unroll
+            for (int slot = 0; slot < E; ++slot) xchg.write(stockham_dest<L, E, R, S>(t, slot), v[slot]);
+            xchg.sync();
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = xchg.read(t + TEAM * e);
+            xchg.sync();
+            pass<INV, P + 1, X>(t, v, xchg);
+        }
+    }
+};
 
 }  // namespace qaf

@@ -21,6 +21,8 @@ col_ifft_kernel(const cplx<real>* __restrict__ spec, cplx<real>* __restrict__ T,
     const int w = threadIdx.x % W, t = threadIdx.x / W;
     const int i = blockIdx.x * W + w;
     XchgCols<real> x{buf, w, W};
+    TeamFFT<real, N, E> fft;
+    fft.template init<N>(t, tw);
     const real s = (real)1 / ((real)N * (real)N);
     cplx<real> v[E];
 #pragma unroll
@@ -37,7 +39,7 @@ col_ifft_kernel(const cplx<real>* __restrict__ spec, cplx<real>* __restrict__ T,
             v[e] = cadd(P0, cmul_i(PH));
         }
     }
-    team_fft<real, N, E, true, N>(t, v, tw, x);
+    fft.template run<true>(t, v, x);
 #pragma unroll
     for (int e = 0; e < E; ++e) T[(size_t)(t + TEAM * e) * H + i] = v[e];
 }
@@ -51,10 +53,12 @@ col_fft_kernel(const cplx<real>* __restrict__ T, cplx<real>* __restrict__ spec, 
     const int w = threadIdx.x % W, t = threadIdx.x / W;
     const int i = blockIdx.x * W + w;
     XchgCols<real> x{buf, w, W};
+    TeamFFT<real, N, E> fft;
+    fft.template init<N>(t, tw);
     cplx<real> v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) v[e] = T[(size_t)(t + TEAM * e) * H + i];
-    team_fft<real, N, E, false, N>(t, v, tw, x);
+    fft.template run<false>(t, v, x);
     // column 0 holds DC + i*Nyquist sequences: unpack with the partner -j
 #pragma unroll
     for (int e = 0; e < E; ++e) x.write(t + TEAM * e, v[e]);
@@ -94,7 +98,9 @@ row_c2r_kernel(const cplx<real>* __restrict__ T, real* __restrict__ phys, const 
             v[e] = cadd(cadd(A, B), cmul_i(cmul(cconj(tw[k]), csub(A, B))));
         }
     }
-    team_fft<real, H, E, true, N>(t, v, tw, x);
+    TeamFFT<real, H, E> fft;
+    fft.template init<N>(t, tw);
+    fft.template run<true>(t, v, x);
     real* o = phys + (size_t)n * N;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -120,7 +126,9 @@ row_r2c_kernel(const real* __restrict__ phys, cplx<real>* __restrict__ T, const 
         const int m = t + TEAM * e;
         v[e] = mk<real>(in[2 * m], in[2 * m + 1]);
     }
-    team_fft<real, H, E, false, N>(t, v, tw, x);
+    TeamFFT<real, H, E> fft;
+    fft.template init<N>(t, tw);
+    fft.template run<false>(t, v, x);
 #pragma unroll
     for (int e = 0; e < E; ++e) x.write(t + TEAM * e, v[e]);
     x.sync();

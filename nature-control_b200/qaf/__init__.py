@@ -36,6 +36,7 @@ EXPORTS = [
     "qaf_xderiv", "qaf_yderiv", "qaf_laplacian", "qaf_vel", "qaf_dealias", "qaf_if_tables", "qaf_integrate",
     "qaf_nonlinear", "qaf_step", "qaf_step_host", "qaf_last_diagnostics", "qaf_check_finite", "qaf_diagnostics",
     "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_state_advance_timed", "qaf_launch_count",
+    "qaf_init_random_q",
 ]
 
 
@@ -120,6 +121,7 @@ def lib():
         L.qaf_state_advance_timed.argtypes = [vp, ctypes.POINTER(CParams), cp, cp, ctypes.POINTER(ctypes.c_double), vp]
         L.qaf_launch_count.argtypes = [vp]
         L.qaf_launch_count.restype = ctypes.c_uint64
+        L.qaf_init_random_q.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -288,6 +290,13 @@ class Mesh:
         cp = p.c()
         _check(lib().qaf_step(self._h, ctypes.byref(cp), integrator, self._chk_spec(w), self._chk_spec(r1),
                               self._chk_spec(r2), nsteps, _stream()))
+        return w, r1, r2
+
+    def random_q(self, seed: int, lo: float = -0.01, hi: float = 0.01):
+        """Seeded initial spectra (w = 0, r1, r2 ~ U(lo, hi); include/qaf_init.h)."""
+        w, r1, r2 = self.new_spec(), self.new_spec(), self.new_spec()
+        _check(lib().qaf_init_random_q(self._h, seed, lo, hi, self._chk_spec(w), self._chk_spec(r1),
+                                       self._chk_spec(r2), _stream()))
         return w, r1, r2
 
     # -- resident state (load once, advance, store snapshots) -----------

@@ -14,7 +14,10 @@ template <typename real, int L, int E, bool INV, int TWN, int P>
 void emulate_pass(std::vector<cplx<real>>& regs, const cplx<real>* tw) {
     using Sc = Sched<L, E>;
     constexpr int R = Sc::radix(P), S = Sc::span(P), TEAM = L / E;
-    for (int t = 0; t < TEAM; ++t) stockham_pass<real, L, E, R, S, INV, TWN>(t, &regs[t * E], tw);
+    // every thread builds its twiddle bases as the kernels do
+    std::vector<TeamFFT<real, L, E>> teams(TEAM);
+    for (int t = 0; t < TEAM; ++t) teams[t].template init<TWN>(t, tw);
+    for (int t = 0; t < TEAM; ++t) stockham_pass_tw<real, L, E, INV, P>(t, &regs[t * E], teams[t].base);
     if constexpr (P + 1 < Sc::passes) {
         std::vector<cplx<real>> buf(L);
         std::vector<int> hit(L, 0);
