@@ -175,6 +175,24 @@ qaf_status qaf_init_random_q(qaf_mesh* mesh, uint64_t seed, double lo, double hi
 qaf_status qaf_diagnostics(qaf_mesh* mesh, const void* w, double* energy, double* enstrophy, double* spectrum,
                            int nshells, void* stream);
 
+/* ---- allocation-free step --------------------------------------------------
+ * No counterpart in the reference (whose Mesh and Field always cudaMalloc).
+ * For callers that cannot allocate device memory when they step — work
+ * recorded into a CUDA graph while a stream is being captured, plug-ins whose
+ * host owns all device memory, real-time loops that must not allocate once
+ * running: the same fused IF-RK step as qaf_step on an n x n grid
+ * (n a power of two, 16 <= n <= 128; lx, ly as in qaf_mesh_desc), in place on
+ * the device spectra w, r1, r2, with every scratch buffer in one fixed 4 MiB
+ * device array inside this library (held by each GPU that loads the library
+ * until the process exits). Larger grids are rejected with QAF_ERR_INVALID.
+ * The first call on a device looks up that array's address with the device
+ * current; make that first call before any stream capture. All calls share the
+ * one array: calls whose work overlaps on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. The array keeps the last
+ * call's contents; each call rebuilds what it needs. */
+qaf_status qaf_step_noalloc(int n, double lx, double ly, qaf_dtype dtype, const qaf_params* p,
+                            qaf_integrator integ, void* w, void* r1, void* r2, int nsteps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -814,3 +815,167 @@ qaf_status qaf_init_random_q(qaf_mesh* m, uint64_t seed, double lo, double hi, v
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free step
+//
+// Some callers cannot allocate device memory at the moment they want to step:
+// code that runs while a stream is being captured into a CUDA graph (where
+// cudaMalloc is not allowed), hosts whose device memory is owned by a pool or
+// arena that a plugin must not bypass, and control loops that must not
+// allocate once they are running. qaf_step_noalloc serves them: it runs the
+// same fused kernels as qaf_step, with all of its scratch — the working copy of
+// the state, the row/column intermediates, twiddles, integrating-factor tables,
+// diagnostics and status flags — in one file-scope device array of fixed size
+// that every GPU loading this library holds until the process exits. The
+// tables are built on the device; nothing is allocated, on the device or on
+// the host, on the success path.
+// ===========================================================================
+namespace {
+
+// Holds the workspace of one grid up to 128 x 128, FP32 or FP64.
+constexpr int kNoAllocMaxN = 128;
+constexpr size_t kNoAllocBytes = 4u << 20;   // 4 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// (with that device current) on the first call made on it.
+constexpr int kMaxDevices = 64;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+std::mutex g_noalloc_mu;
+
+qaf_status noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    QAF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(QAF_ERR_UNSUPPORTED, "qaf_step_noalloc: device index out of range");
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        unsigned char* ptr = nullptr;
+        QAF_CUDA(cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = ptr;
+    }
+    *out = g_noalloc_ptr[dev];
+    return QAF_OK;
+}
+
+// Workspace element layout inside the fixed array (the same buffers that
+// ensure_ws allocates for a mesh), in complex elements of the precision.
+template <typename real>
+size_t noalloc_carve(Workspace<real>& w, cplx<real>* b, int N) {
+    const int H = N / 2;
+    const size_t plane = (size_t)N * H;
+    size_t off = 0;
+    auto take = [&](size_t n) { size_t o = off; off += align_up(n); return o; };
+    for (int f = 0; f < 3; ++f) { w.old_m[f] = b + take(plane); w.old_n[f] = b + take(N); }
+    for (int f = 0; f < 3; ++f) { w.acc_m[f] = b + take(plane); w.acc_n[f] = b + take(N); }
+    w.Y = b + take(NY * plane);
+    w.D = b + take((size_t)PF_COUNT * N);
+    w.G = b + take(NG * plane);
+    w.Ed = b + take((size_t)NE * N);
+    w.T = b + take(plane);
+    w.tw = b + take(N);
+    w.ex = reinterpret_cast<real*>(b + take((4 * (H + 1) + 1) / 2 + 1));
+    w.ey = reinterpret_cast<real*>(b + take((4 * N + 1) / 2 + 1));
+    w.diag = reinterpret_cast<double*>(b + take(4 * sizeof(double) / sizeof(cplx<real>) + 1));
+    w.flags = reinterpret_cast<unsigned*>(b + take(1));
+    w.block = b;
+    w.N = N;
+    return off * sizeof(cplx<real>);
+}
+
+// Twiddles exp(-2 pi i m / N) and the separable integrating factors, built on
+// the device (sincospi / exp in double, rounded to the working precision).
+template <typename real>
+__global__ void noalloc_tables_kernel(cplx<real>* tw, real* ex, real* ey, int N, double dkx, double dky, double dt,
+                                      double re) {
+    const int H = N / 2;
+    const int total = N + 4 * (H + 1) + 4 * N;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        if (k < N) {
+            double sn, cs;
+            sincospi(-2.0 * (double)k / (double)N, &sn, &cs);
+            tw[k] = mk<real>((real)cs, (real)sn);
+            continue;
+        }
+        const bool is_x = k < N + 4 * (H + 1);
+        const int r = is_x ? k - N : k - N - 4 * (H + 1);
+        const int per = is_x ? H + 1 : N;
+        const int c = r / per, idx = r % per;
+        const double step = (c == 0 || c == 2) ? dt : 0.5 * dt;
+        const double visc = c < 2 ? 1.0 / re : 1.0;
+        const double kk = is_x ? dkx * idx : dky * (idx < N / 2 + 1 ? idx : idx - N);
+        const real val = (real)exp(-visc * kk * kk * step);
+        if (is_x) ex[r] = val; else ey[r] = val;
+    }
+}
+
+struct OpStepNoAlloc {
+    template <typename real, int N>
+    static qaf_status run(qaf_mesh* m, unsigned char* scratch, const qaf_params* p, int integ, void* const* state,
+                          int nsteps, cudaStream_t st) {
+        if (N > kNoAllocMaxN) return fail(QAF_ERR_INVALID, "qaf_step_noalloc: grid larger than 128 x 128");
+        Workspace<real>& w = ws<real>(m);
+        const size_t need = noalloc_carve<real>(w, reinterpret_cast<cplx<real>*>(scratch), N);
+        if (need > kNoAllocBytes) return fail(QAF_ERR_INVALID, "qaf_step_noalloc: workspace exceeds the fixed scratch");
+        QAF_TRY((Launch<real, N>::setup()));
+        noalloc_tables_kernel<real><<<8, 256, 0, st>>>(w.tw, w.ex, w.ey, N, m->dkx, m->dky, p->dt, p->re);
+        // the array keeps the previous call's contents: clear the status flags
+        QAF_CUDA(cudaMemsetAsync(w.flags, 0, sizeof(unsigned), st));
+        w.e0[0] = (real)exp(-p->rf / p->re * p->dt);
+        w.e0[1] = (real)exp(-p->rf / p->re * p->dt * 0.5);
+        w.e0[2] = (real)exp(p->q_lin * p->dt);
+        w.e0[3] = (real)exp(p->q_lin * p->dt * 0.5);
+        for (int f = 0; f < 3; ++f)
+            ref_to_internal<real><<<grid_for(spec_elems(m)), 256, 0, st>>>(
+                reinterpret_cast<const cplx<real>*>(state[f]), w.old_m[f], w.old_n[f], N);
+        StageArgs<real> a = make_args<real>(m, p);
+        a.integrator = integ;
+        const int nst = integ == QAF_IFRK4 ? 4 : (integ == QAF_IFRK2 ? 2 : 1);
+        a.mode = MODE_PROLOGUE;
+        a.do_inverse = 1;
+        Launch<real, N>::col(a, st);
+        a.mode = MODE_STAGE;
+        for (int s = 0; s < nsteps; ++s) {
+            const bool last_step = s == nsteps - 1;
+            if (last_step) QAF_CUDA(cudaMemsetAsync(w.diag, 0, 2 * sizeof(double), st));
+            for (int k = 1; k <= nst; ++k) {
+                a.stage = k;
+                a.last_stage = k == nst;
+                a.do_inverse = !(last_step && k == nst);
+                a.diag = (last_step && k == nst) ? w.diag : nullptr;
+                Launch<real, N>::row(a, st);
+                Launch<real, N>::col(a, st);
+            }
+        }
+        for (int f = 0; f < 3; ++f)
+            from_internal<real>(m, w.old_m[f], w.old_n[f], state[f], st);
+        return post_launch("qaf_step_noalloc");
+    }
+};
+
+}  // namespace
+
+extern "C" qaf_status qaf_step_noalloc(int n, double lx, double ly, qaf_dtype dtype, const qaf_params* p,
+                                       qaf_integrator integ, void* w, void* r1, void* r2, int nsteps, void* stream) {
+    if (!p || !w || !r1 || !r2) return fail(QAF_ERR_INVALID, "qaf_step_noalloc: null pointer");
+    if (n < 16 || n > kNoAllocMaxN || (n & (n - 1)))
+        return fail(QAF_ERR_INVALID, "qaf_step_noalloc: n must be a power of two in [16, 128] "
+                                     "(the fixed scratch holds the workspace of a 128 x 128 grid)");
+    if (dtype != QAF_F32 && dtype != QAF_F64) return fail(QAF_ERR_INVALID, "qaf_step_noalloc: bad dtype");
+    if (!(lx > 0) || !(ly > 0)) return fail(QAF_ERR_INVALID, "qaf_step_noalloc: lx, ly must be positive");
+    QAF_TRY(check_params(p));
+    if (integ != QAF_IFE && integ != QAF_IFRK2 && integ != QAF_IFRK4) return fail(QAF_ERR_INVALID, "bad integrator");
+    if (nsteps < 0) return fail(QAF_ERR_INVALID, "nsteps < 0");
+    if (nsteps == 0) return QAF_OK;
+    unsigned char* scratch = nullptr;
+    QAF_TRY(noalloc_scratch(&scratch));
+    // a mesh description on the stack whose workspace points into the fixed array
+    qaf_mesh m;
+    m.desc = qaf_mesh_desc{n, n, lx, ly, dtype};
+    m.nxh = n / 2 + 1;
+    m.dkx = 2 * M_PI / lx;
+    m.dky = 2 * M_PI / ly;
+    m.device = 0;
+    void* st[3] = {w, r1, r2};
+    return dispatch<OpStepNoAlloc>(&m, &m, scratch, p, (int)integ, (void* const*)st, nsteps, (cudaStream_t)stream);
+}

@@ -36,7 +36,7 @@ EXPORTS = [
     "qaf_xderiv", "qaf_yderiv", "qaf_laplacian", "qaf_vel", "qaf_dealias", "qaf_if_tables", "qaf_integrate",
     "qaf_nonlinear", "qaf_step", "qaf_step_host", "qaf_last_diagnostics", "qaf_check_finite", "qaf_diagnostics",
     "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_state_advance_timed", "qaf_launch_count",
-    "qaf_init_random_q",
+    "qaf_init_random_q", "qaf_step_noalloc",
 ]
 
 
@@ -122,6 +122,8 @@ def lib():
         L.qaf_launch_count.argtypes = [vp]
         L.qaf_launch_count.restype = ctypes.c_uint64
         L.qaf_init_random_q.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp]
+        L.qaf_step_noalloc.argtypes = [cp, ctypes.c_double, ctypes.c_double, cp, ctypes.POINTER(CParams), cp,
+                                       vp, vp, vp, cp, vp]
         _lib = L
     return _lib
 
