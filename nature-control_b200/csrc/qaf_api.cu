@@ -2,6 +2,8 @@
 // configuration per grid size and precision, and the step driver.
 #include "qaf.h"
 #include "qaf_init.h"
+
+#include <cudaTypedefs.h>   // PFN_cuTensorMapEncodeTiled
 #include "qaf_kernels.cuh"
 #include "qaf_ops.cuh"
 
@@ -37,6 +39,18 @@ qaf_status fail(qaf_status st, const std::string& msg) {
     } while (0)
 
 bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// Launch-shape defaults (values per thread of the column / row FFTs, threads
+// per row-kernel CTA); overridable at build time for tuning.
+#ifndef QAF_COL_E
+#define QAF_COL_E 8
+#endif
+#ifndef QAF_ROW_E
+#define QAF_ROW_E 8
+#endif
+#ifndef QAF_ROW_THREADS
+#define QAF_ROW_THREADS 256
+#endif
 constexpr int kMinN = 16, kMaxN = 1024;
 
 // ---------------------------------------------------------------------------
@@ -48,22 +62,25 @@ struct Cfg {
     static constexpr bool F32 = sizeof(real) == 4;
     // CTAs per SM the register budget is sized for (FP64 kernels need > 128 registers)
     static constexpr int MINB = F32 ? 2 : 1;
-    // column kernel: W kx-columns per CTA, EC values per thread of a length-N y-FFT
-    static constexpr int W = 4 < H ? 4 : H;
-    static constexpr int EC = 16 < N ? 16 : N;
-    static constexpr int COL_THREADS = W * (N / EC);
-    static constexpr size_t COL_SMEM = (size_t)(W * N + 2 * N) * sizeof(cplx<real>);
-    static constexpr int COL_BLOCKS = 3 * (H / W) + 3;
+    // column kernel (persistent): a tile of TW kx-columns per work item, EC values
+    // per thread of a length-N y-FFT
+    static constexpr int EC = QAF_COL_E < N ? QAF_COL_E : N;
+    static constexpr int COL_THREADS = TW * (N / EC);
+    static constexpr size_t COL_SMEM = ColKernel<real, N, EC>::SMEM;
+    static constexpr int COL_ITEMS = ColKernel<real, N, EC>::NITEMS;
     // row kernel: ER values per thread of a length-N x-FFT, ROWS rows per CTA
-    static constexpr int ER = 8 < N ? 8 : N;
+    static constexpr int ER = QAF_ROW_E < N ? QAF_ROW_E : N;
     static constexpr int TEAM_R = N / ER;
-    static constexpr int ROWS_A = 256 / TEAM_R > 0 ? 256 / TEAM_R : 1;
+    static constexpr int ROWS_A = QAF_ROW_THREADS / TEAM_R > 0 ? QAF_ROW_THREADS / TEAM_R : 1;
     static constexpr int ROWS_B = N / 8 > 0 ? N / 8 : 1;
     static constexpr int ROWS = ROWS_A < ROWS_B ? ROWS_A : ROWS_B;
     static constexpr int ROW_THREADS = ROWS * TEAM_R;
     static constexpr size_t ROW_SMEM = RowKernel<real, N, ER, ROWS>::SMEM;
     static constexpr int ROW_BLOCKS = N / ROWS;
-    // standalone transforms: half-length row FFTs
+    // standalone transforms: W kx-columns per CTA, half-length row FFTs
+    static constexpr int W = 4 < H ? 4 : H;
+    static constexpr int COLT_THREADS = W * (N / EC);
+    static constexpr size_t COLT_SMEM = (size_t)W * N * sizeof(cplx<real>);
     static constexpr int ERT = (F32 ? 8 : 4) < H ? (F32 ? 8 : 4) : H;
     static constexpr int TEAM_T = H / ERT;
     static constexpr int ROWS_T = (TEAM_T >= 128) ? 1 : (128 / TEAM_T <= N ? 128 / TEAM_T : N);
@@ -90,11 +107,38 @@ struct Workspace {
     real* ey;
     double* diag;      // [0] energy sum, [1] enstrophy sum, [2..] spectrum shells (scratch)
     unsigned* flags;
+    int* queue;        // work counter of the persistent column kernel
+    CUtensorMap tm_G;  // TMA view of the G arrays
     double cached[5] = {NAN, NAN, NAN, NAN, NAN};   // dt, re, rf, q_lin, unused -> IF tables valid for
     real e0[4];
 };
 
 size_t align_up(size_t x) { return (x + 31) & ~size_t(31); }
+
+// TMA descriptor of the G arrays: [NG*N rows][H columns] of 8-byte elements
+// (two per FP64 complex), boxes of TW columns x min(N, 256) rows.
+template <typename real>
+qaf_status encode_g_map(CUtensorMap* tm, const cplx<real>* G, int N) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        QAF_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) return fail(QAF_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const int H = N / 2;
+    const cuuint64_t cpe = sizeof(cplx<real>) / 8;
+    cuuint64_t dims[2] = {(cuuint64_t)H * cpe, (cuuint64_t)NG * N};
+    cuuint64_t strides[1] = {(cuuint64_t)H * cpe * 8};
+    cuuint32_t box[2] = {(cuuint32_t)(TW * cpe), (cuuint32_t)(N < 256 ? N : 256)};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<cplx<real>*>(G), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(QAF_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return QAF_OK;
+}
 
 }  // namespace
 
@@ -135,6 +179,7 @@ qaf_status ensure_ws(qaf_mesh* m) {
     size_t oex = take((4 * (H + 1) + 1) / 2 + 1), oey = take((4 * N + 1) / 2 + 1);
     size_t odiag = take((4 + 512 + 513) * sizeof(double) / sizeof(cplx<real>) + 1);
     size_t oflags = take(1);
+    size_t oqueue = take(1);
     cplx<real>* b = nullptr;
     cudaError_t e = cudaMalloc((void**)&b, off * sizeof(cplx<real>));
     if (e != cudaSuccess) return fail(QAF_ERR_ALLOC, std::string("workspace cudaMalloc: ") + cudaGetErrorString(e));
@@ -149,6 +194,7 @@ qaf_status ensure_ws(qaf_mesh* m) {
     w.ey = reinterpret_cast<real*>(b + oey);
     w.diag = reinterpret_cast<double*>(b + odiag);
     w.flags = reinterpret_cast<unsigned*>(b + oflags);
+    w.queue = reinterpret_cast<int*>(b + oqueue);
     // twiddles exp(-2 pi i m / N) from long double
     std::vector<cplx<real>> tw(N);
     const long double pi = 3.141592653589793238462643383279502884L;
@@ -157,6 +203,7 @@ qaf_status ensure_ws(qaf_mesh* m) {
         tw[k] = mk<real>((real)cosl(a), (real)sinl(a));
     }
     QAF_CUDA(cudaMemcpy(w.tw, tw.data(), N * sizeof(cplx<real>), cudaMemcpyHostToDevice));
+    QAF_TRY(encode_g_map<real>(&w.tm_G, w.G, N));
     QAF_CUDA(cudaMemset(w.flags, 0, sizeof(unsigned)));
     QAF_CUDA(cudaMemset(w.diag, 0, 2 * sizeof(double)));
     return QAF_OK;
@@ -212,7 +259,8 @@ StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
     }
     a.Y = w.Y; a.D = w.D; a.G = w.G; a.Ed = w.Ed; a.tw = w.tw; a.ex = w.ex; a.ey = w.ey;
     for (int c = 0; c < 4; ++c) a.e0[c] = w.e0[c];
-    a.diag = w.diag; a.flags = w.flags;
+    a.diag = w.diag; a.flags = w.flags; a.queue = w.queue;
+    a.tm_G = w.tm_G;
     return a;
 }
 
@@ -222,29 +270,37 @@ StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
 template <typename real, int N>
 struct Launch {
     using C = Cfg<real, N>;
+    static inline int col_blocks = 0;   // persistent grid: resident CTAs, at most the item count
     static qaf_status setup() {
         static bool done = false;
         if (done) return QAF_OK;
-        QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::W, C::EC, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::EC, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
         QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::ROW_SMEM));
-        QAF_CUDA(cudaFuncSetAttribute(col_ifft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
-        QAF_CUDA(cudaFuncSetAttribute(col_fft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(col_ifft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(col_fft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
+        int dev = 0, sms = 0, per_sm = 0;
+        QAF_CUDA(cudaGetDevice(&dev));
+        QAF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        QAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_kernel<real, N, C::EC, C::MINB>,
+                                                               C::COL_THREADS, C::COL_SMEM));
+        if (per_sm < 1) return fail(QAF_ERR_UNSUPPORTED, "column kernel does not fit on an SM");
+        col_blocks = sms * per_sm < C::COL_ITEMS ? sms * per_sm : C::COL_ITEMS;
         done = true;
         return QAF_OK;
     }
     static void col(const StageArgs<real>& a, cudaStream_t st) {
-        col_kernel<real, N, C::W, C::EC, C::MINB><<<C::COL_BLOCKS, C::COL_THREADS, C::COL_SMEM, st>>>(a);
+        col_kernel<real, N, C::EC, C::MINB><<<col_blocks, C::COL_THREADS, C::COL_SMEM, st>>>(a);
     }
     static void row(const StageArgs<real>& a, cudaStream_t st) {
         row_kernel<real, N, C::ER, C::ROWS, C::MINB><<<C::ROW_BLOCKS, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
     }
     static void bwd(const cplx<real>* spec, cplx<real>* T, real* phys, const cplx<real>* tw, cudaStream_t st) {
-        col_ifft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COL_THREADS, C::COL_SMEM, st>>>(spec, T, tw);
+        col_ifft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COLT_THREADS, C::COLT_SMEM, st>>>(spec, T, tw);
         row_c2r_kernel<real, N, C::ERT, C::ROWS_T><<<C::ROWT_BLOCKS, C::ROWT_THREADS, C::ROWT_SMEM, st>>>(T, phys, tw);
     }
     static void fwd(const real* phys, cplx<real>* T, cplx<real>* spec, const cplx<real>* tw, cudaStream_t st) {
         row_r2c_kernel<real, N, C::ERT, C::ROWS_T><<<C::ROWT_BLOCKS, C::ROWT_THREADS, C::ROWT_SMEM, st>>>(phys, T, tw);
-        col_fft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COL_THREADS, C::COL_SMEM, st>>>(T, spec, tw);
+        col_fft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COLT_THREADS, C::COLT_SMEM, st>>>(T, spec, tw);
     }
 };
 
@@ -258,7 +314,11 @@ qaf_status dispatch(const qaf_mesh* m, A&&... args) {
         return f64 ? F::template run<double, n>(std::forward<A>(args)...)                \
                    : F::template run<float, n>(std::forward<A>(args)...);
     switch (N) {
+#ifdef QAF_ONLY_N
+        QAF_CASE(QAF_ONLY_N)
+#else
         QAF_CASE(16) QAF_CASE(32) QAF_CASE(64) QAF_CASE(128) QAF_CASE(256) QAF_CASE(512) QAF_CASE(1024)
+#endif
         default: break;
     }
 #undef QAF_CASE
@@ -333,6 +393,7 @@ struct OpNonlinear {
         StageArgs<real> a = make_args<real>(m, p);
         a.phys_out = static_cast<real*>(phys_out);
         a.mode = MODE_PROLOGUE; a.do_inverse = 1;
+        QAF_CUDA(cudaMemsetAsync(w.queue, 0, sizeof(int), st));
         Launch<real, N>::col(a, st);
         Launch<real, N>::row(a, st);
         a.mode = MODE_NONL; a.do_inverse = 0;
@@ -396,6 +457,7 @@ struct OpAdvance {
         };
         if (!m->y_valid) {
             a.mode = MODE_PROLOGUE; a.do_inverse = 1;
+            QAF_CUDA(cudaMemsetAsync(w.queue, 0, sizeof(int), st));
             Launch<real, N>::col(a, st);
             m->launches += 1;
         }
@@ -760,6 +822,7 @@ qaf_status qaf_last_diagnostics(qaf_mesh* m, double out[2]) {
     const double n4 = (double)m->desc.nx * m->desc.ny * (double)m->desc.nx * m->desc.ny;
     out[0] = 0.5 * h[1] / n4;   // energy: sum |w|^2 / k^2
     out[1] = 0.5 * h[0] / n4;   // enstrophy: sum |w|^2
+    if (flags & FLAG_WAIT_TIMEOUT) return fail(QAF_ERR_CUDA, "a kernel's wait for its own copy timed out");
     if (flags) return fail(QAF_ERR_NONFINITE, "a step produced a non-finite value");
     return QAF_OK;
 }
@@ -772,6 +835,7 @@ qaf_status qaf_check_finite(qaf_mesh* m, void* stream) {
     unsigned flags = 0;
     QAF_CUDA(cudaMemcpy(&flags, fp, sizeof(flags), cudaMemcpyDeviceToHost));
     QAF_CUDA(cudaMemset(fp, 0, sizeof(unsigned)));
+    if (flags & FLAG_WAIT_TIMEOUT) return fail(QAF_ERR_CUDA, "a kernel's wait for its own copy timed out");
     if (flags) return fail(QAF_ERR_NONFINITE, "a step produced a non-finite value");
     return QAF_OK;
 }
@@ -878,6 +942,7 @@ size_t noalloc_carve(Workspace<real>& w, cplx<real>* b, int N) {
     w.ey = reinterpret_cast<real*>(b + take((4 * N + 1) / 2 + 1));
     w.diag = reinterpret_cast<double*>(b + take(4 * sizeof(double) / sizeof(cplx<real>) + 1));
     w.flags = reinterpret_cast<unsigned*>(b + take(1));
+    w.queue = reinterpret_cast<int*>(b + take(1));
     w.block = b;
     w.N = N;
     return off * sizeof(cplx<real>);
@@ -917,6 +982,7 @@ struct OpStepNoAlloc {
         Workspace<real>& w = ws<real>(m);
         const size_t need = noalloc_carve<real>(w, reinterpret_cast<cplx<real>*>(scratch), N);
         if (need > kNoAllocBytes) return fail(QAF_ERR_INVALID, "qaf_step_noalloc: workspace exceeds the fixed scratch");
+        QAF_TRY(encode_g_map<real>(&w.tm_G, w.G, N));
         QAF_TRY((Launch<real, N>::setup()));
         noalloc_tables_kernel<real><<<8, 256, 0, st>>>(w.tw, w.ex, w.ey, N, m->dkx, m->dky, p->dt, p->re);
         // the array keeps the previous call's contents: clear the status flags
@@ -933,6 +999,7 @@ struct OpStepNoAlloc {
         const int nst = integ == QAF_IFRK4 ? 4 : (integ == QAF_IFRK2 ? 2 : 1);
         a.mode = MODE_PROLOGUE;
         a.do_inverse = 1;
+        QAF_CUDA(cudaMemsetAsync(w.queue, 0, sizeof(int), st));
         Launch<real, N>::col(a, st);
         a.mode = MODE_STAGE;
         for (int s = 0; s < nsteps; ++s) {

@@ -12,124 +12,268 @@ template <typename P>
 __device__ __forceinline__ P pick3(const P (&arr)[3], int f) { return f == 0 ? arr[0] : (f == 1 ? arr[1] : arr[2]); }
 
 // ---------------------------------------------------------------------------
-// Column kernel, regular tiles: W packed kx-columns i of field f.
+// TMA bulk copies (cp.async.bulk) into shared memory, completed on an mbarrier.
+// Waits are bounded: a wait that runs out sets FLAG_WAIT_TIMEOUT and returns,
+// so a copy that never lands cannot hang the GPU (the data is then garbage and
+// the status tells the host).
 // ---------------------------------------------------------------------------
-template <typename real, int N, int W, int E>
-__device__ __forceinline__ void col_regular(const StageArgs<real>& a, int f, int i, int t, int w, cplx<real>* buf) {
-    constexpr int H = N / 2, TEAM = N / E;
-    XchgCols<real> x{buf, w, W};
-    TeamFFT<real, N, E> fft;
-    fft.template init<N>(t, a.tw);
-    const real kx = a.dkx * (real)i;
-    const real s = (real)1 / ((real)N * (real)N);
-    const bool edge_col = (i == 0);   // packed column 0 belongs to the edge CTA
-    cplx<real> v[E], nl[E], curr[E];
-    const size_t plane = (size_t)N * H;
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-    if (a.mode != MODE_PROLOGUE) {
-        const int gbase = f == 0 ? 0 : (f == 1 ? 3 : 5);
-        const int ng = f == 0 ? 3 : 2;
-#pragma unroll
-        for (int e = 0; e < E; ++e) nl[e] = mk<real>(0, 0);
-#pragma unroll 1
-        for (int g = 0; g < ng; ++g) {
-            const cplx<real>* G = a.G + (size_t)(gbase + g) * plane;
-#pragma unroll
-            for (int e = 0; e < E; ++e) v[e] = G[(size_t)(t + TEAM * e) * H + i];
-            fft.template run<false>(t, v, x);
-#pragma unroll
-            for (int e = 0; e < E; ++e) {
-                const real ky = ky_of<real>(t + TEAM * e, N, a.dky);
-                const real m = g == 0 ? (real)1 : (g == 1 ? ky : ky * ky);
-                nl[e] = cadd(nl[e], cscale(v[e], m));
-            }
-        }
-        if (a.mode == MODE_NONL) {
-            if (!edge_col)
-#pragma unroll
-                for (int e = 0; e < E; ++e) pick3(a.nl_m, f)[(size_t)(t + TEAM * e) * H + i] = nl[e];
-            return;
-        }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    // order this thread's earlier generic-proxy accesses to dst before the async-proxy write
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}"
+                 ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+// 2D tiled TMA load of a box at element coordinates (x, y) of tensor map tm;
+// the transaction bytes were announced on bar by the caller
+__device__ __forceinline__ void tile_load_2d(void* dst, const CUtensorMap* tm, int x, int y, uint64_t* bar) {
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                 ::"r"(smem_u32(dst)), "l"(tm), "r"(x), "r"(y), "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}"
+                 ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned* flags) {
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (flags) atomicOr(flags, FLAG_WAIT_TIMEOUT);
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Column kernel (persistent). Work items, largest first:
+//   [0, TILES)            the r1 and r2 columns of tile T (4 + 4 y-FFTs)
+//   [TILES, 2 TILES)      the w columns of tile T (3 + 4 y-FFTs)
+//   [2 TILES, 2 TILES+3)  the kx = 0 / kx = N/2 edge columns of field f
+// A tile is TW kx-columns over all N rows, one contiguous slab of each array.
+// Every slab an item reads (G arrays, old, acc) is fetched by one TMA bulk
+// copy into a ring of three shared-memory buffers, issued up to three slabs
+// ahead; a y-FFT runs in the buffer its input arrived in.
+// ---------------------------------------------------------------------------
+template <typename real, int N, int E>
+struct ColKernel {
+    static constexpr int H = N / 2, TEAM = N / E, TILES = H / TW, NTHREADS = TW * TEAM;
+    static constexpr int NITEMS = 2 * TILES + 3;
+    static constexpr size_t SLAB = (size_t)N * TW;   // complex elements of one slab
+    static constexpr int BOXR = N < 256 ? N : 256;    // rows per TMA box (at most 256)
+    static constexpr size_t SMEM = 3 * SLAB * sizeof(cplx<real>) + 2 * N * sizeof(cplx<real>) + 4 * sizeof(uint64_t) + 16;
+    using FFT = TeamFFT<real, N, E>;
+
+    const StageArgs<real>& a;
+    const FFT& fft;
+    int t, w;
+    cplx<real>* bufs;      // three slab buffers back to back
+    uint64_t* mbar;        // one mbarrier per buffer
+    unsigned parity;       // bit b: parity of buffer b's latest issue
+    // the current item: fields fa (and fb), tile T; slab sequence per field:
+    // its G arrays (none in the prologue), then old and/or acc
+    int fa, fb, T, nseq, next, per_a;
+    bool need_old, need_acc;
+
+    __device__ cplx<real>* buf(int b) const { return bufs + (size_t)b * SLAB; }
+    __device__ int nG(int f) const { return a.mode == MODE_PROLOGUE ? 0 : (f == 0 ? 3 : 2); }
+    __device__ int per_field(int f) const { return nG(f) + (need_old ? 1 : 0) + (need_acc ? 1 : 0); }
+    // slab sidx of the item: a G array (>= 0: its plane index) or a state slab (pointer)
+    __device__ int slab_g(int sidx) const {
+        const int f = sidx < per_a ? fa : fb;
+        const int r = sidx < per_a ? sidx : sidx - per_a;
+        return r < nG(f) ? (f == 0 ? 0 : (f == 1 ? 3 : 5)) + r : -1;
     }
-
-    // stage update
-    const bool need_old = a.mode == MODE_PROLOGUE || a.integrator == INT_IFE ||
-                          (a.integrator == INT_IFRK4 && a.stage <= 3) || (a.integrator == INT_IFRK2 && a.stage == 1);
-    const bool need_acc = a.mode == MODE_STAGE && ((a.integrator == INT_IFRK4 && a.stage >= 2) ||
-                                                   (a.integrator == INT_IFRK2 && a.stage == 2));
-    cplx<real>* om = pick3(a.old_m, f);
-    cplx<real>* am = pick3(a.acc_m, f);
-    double zsum = 0, esum = 0;
-    bool bad = false;
-    if (a.mode == MODE_PROLOGUE) {
-#pragma unroll
-        for (int e = 0; e < E; ++e) curr[e] = om[(size_t)(t + TEAM * e) * H + i];
-    } else {
-        const int cls = f == 0 ? 0 : 2;
-        const real exf = a.ex[cls * (H + 1) + i] * a.e0[cls];
-        const real exh = a.ex[(cls + 1) * (H + 1) + i] * a.e0[cls + 1];
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int j = t + TEAM * e;
-            const size_t idx = (size_t)j * H + i;
-            const real Ef = exf * a.ey[cls * N + j];
-            const real Eh = exh * a.ey[(cls + 1) * N + j];
-            const cplx<real> o = need_old ? om[idx] : mk<real>(0, 0);
-            const cplx<real> ac = need_acc ? am[idx] : mk<real>(0, 0);
-            StageUpdate<real> u = stage_update(a, nl[e], o, ac, Ef, Eh, mask_keep(a, i, j));
-            if (!edge_col) {
-                if (u.write_acc) am[idx] = u.acc;
-                if (u.write_old) {
-                    om[idx] = u.acc;
-                    bad |= !(isfinite(u.acc.x) && isfinite(u.acc.y));
-                    if (f == 0 && a.diag) {
-                        const real ky = ky_of<real>(j, N, a.dky);
-                        const double k2 = (double)kx * kx + (double)ky * ky;
-                        const double m2 = (double)u.acc.x * u.acc.x + (double)u.acc.y * u.acc.y;
-                        zsum += 2.0 * m2;
-                        if (k2 > 0) esum += 2.0 * m2 / k2;
-                    }
+    __device__ const cplx<real>* slab_state(int sidx) const {
+        const int f = sidx < per_a ? fa : fb;
+        const int r = sidx < per_a ? sidx : sidx - per_a;
+        const size_t base = (size_t)T * SLAB;
+        if (r == nG(f) && need_old) return pick3(a.old_m, f) + base;
+        return pick3(a.acc_m, f) + base;
+    }
+    // issue every slab with index < k that has not been issued yet: G arrays
+    // (row-major [n][k]) as TMA boxes of TW columns x BOXR rows, state slabs
+    // (column-tiled, contiguous) as one bulk copy
+    __device__ void issue_upto(int k) {
+        if (k > nseq) k = nseq;
+        while (next < k) {
+            const int b = next % 3;
+            __syncthreads();   // every thread is done with buffer b
+            if (threadIdx.x == 0) {
+                const unsigned bytes = (unsigned)(SLAB * sizeof(cplx<real>));
+                const int g = slab_g(next);
+                if (g >= 0) {
+                    expect_tx(&mbar[b], bytes);
+                    constexpr int CPE = sizeof(cplx<real>) / 8;   // 8-byte elements per complex
+#pragma unroll 1
+                    for (int r0 = 0; r0 < N; r0 += BOXR)
+                        tile_load_2d(buf(b) + (size_t)r0 * TW, &a.tm_G, T * TW * CPE, g * N + r0, &mbar[b]);
+                } else {
+                    bulk_load(buf(b), slab_state(next), bytes, &mbar[b]);
                 }
             }
-            curr[e] = u.curr;
-        }
-        if (a.last_stage) {
-            // CTAs of the smallest grids hold partial warps: reduce with warp
-            // shuffles only when every warp is full
-            const bool full_warps = (blockDim.x & 31) == 0;
-            if (full_warps) {
-                if (a.flags && __any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(a.flags, 1u);
-                if (f == 0 && a.diag) {
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        zsum += __shfl_xor_sync(0xffffffffu, zsum, o);
-                        esum += __shfl_xor_sync(0xffffffffu, esum, o);
-                    }
-                    if ((threadIdx.x & 31) == 0) { atomicAdd(&a.diag[0], zsum); atomicAdd(&a.diag[1], esum); }
-                }
-            } else {
-                if (a.flags && bad) atomicOr(a.flags, 1u);
-                if (f == 0 && a.diag) { atomicAdd(&a.diag[0], zsum); atomicAdd(&a.diag[1], esum); }
-            }
+            parity ^= 1u << b;
+            ++next;
         }
     }
+    __device__ cplx<real>* wait(int sidx) {
+        const int b = sidx % 3;
+        mbar_wait(&mbar[b], ((parity >> b) & 1u) ^ 1u, a.flags);
+        return buf(b);
+    }
 
-    if (!a.do_inverse) return;
-    const int nq = f == 0 ? 4 : 2;
-#pragma unroll 1
-    for (int qq = 0; qq < nq; ++qq) {
-        const int q = f == 0 ? (qq == 0 ? 0 : qq + 2) : (f == 1 ? (qq == 0 ? 1 : 6) : (qq == 0 ? 2 : 7));
+    // forward y-FFT of slab sidx; adds ky^pow * F_y(G) to nl
+    __device__ void forward(int sidx, int pow, cplx<real> (&nl)[E]) {
+        cplx<real>* b = wait(sidx);
+        XchgCols<real> x{b, w, TW};
+        cplx<real> v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = b[(t + TEAM * e) * TW + w];
+        x.sync();
+        fft.template run<false>(t, v, x);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const real ky = ky_of<real>(t + TEAM * e, N, a.dky);
-            v[e] = y_mult<real>(q, curr[e], ky, kx * kx + ky * ky, s);
+            const real m = pow == 0 ? (real)1 : (pow == 1 ? ky : ky * ky);
+            nl[e] = cadd(nl[e], cscale(v[e], m));
         }
-        fft.template run<true>(t, v, x);
-        cplx<real>* Y = a.Y + (size_t)q * plane;
-#pragma unroll
-        for (int e = 0; e < E; ++e) Y[(size_t)(t + TEAM * e) * H + i] = v[e];
+        issue_upto(sidx + 4);
     }
-}
+
+    // field f of the current tile; its slabs start at s0
+    __device__ void field(int f, int s0) {
+        const int i = T * TW + w;
+        const bool edge_col = (i == 0);   // kx = 0 belongs to the edge item
+        const real kx = a.dkx * (real)i;
+        const real sc = (real)1 / ((real)N * (real)N);
+        const int ng = nG(f);
+        const size_t base = (size_t)T * SLAB;
+        cplx<real> nl[E], curr[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) nl[e] = mk<real>(0, 0);
+        for (int g = 0; g < ng; ++g) forward(s0 + g, g, nl);
+
+        if (a.mode == MODE_NONL) {
+            cplx<real>* out = pick3(a.nl_m, f) + base;
+            if (!edge_col)
+#pragma unroll
+                for (int e = 0; e < E; ++e) out[(t + TEAM * e) * TW + w] = nl[e];
+            return;
+        }
+        // stage update, old and acc read from their slabs
+        const int so = s0 + ng, sa = so + (need_old ? 1 : 0);
+        const cplx<real>* ob = need_old ? wait(so) : nullptr;
+        const cplx<real>* ab = need_acc ? wait(sa) : nullptr;
+        cplx<real>* om = pick3(a.old_m, f) + base;
+        cplx<real>* am = pick3(a.acc_m, f) + base;
+        double zsum = 0, esum = 0;
+        bool bad = false;
+        if (a.mode == MODE_PROLOGUE) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) curr[e] = ob[(t + TEAM * e) * TW + w];
+        } else {
+            const int cls = f == 0 ? 0 : 2;
+            const real exf = a.ex[cls * (H + 1) + i] * a.e0[cls];
+            const real exh = a.ex[(cls + 1) * (H + 1) + i] * a.e0[cls + 1];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int j = t + TEAM * e;
+                const int li = j * TW + w;
+                const real Ef = exf * a.ey[cls * N + j];
+                const real Eh = exh * a.ey[(cls + 1) * N + j];
+                const cplx<real> o = need_old ? ob[li] : mk<real>(0, 0);
+                const cplx<real> ac = need_acc ? ab[li] : mk<real>(0, 0);
+                StageUpdate<real> u = stage_update(a, nl[e], o, ac, Ef, Eh, mask_keep(a, i, j));
+                if (!edge_col) {
+                    if (u.write_acc) am[li] = u.acc;
+                    if (u.write_old) {
+                        om[li] = u.acc;
+                        bad |= !(isfinite(u.acc.x) && isfinite(u.acc.y));
+                        if (f == 0 && a.diag) {
+                            const real ky = ky_of<real>(j, N, a.dky);
+                            const double k2 = (double)kx * kx + (double)ky * ky;
+                            const double m2 = (double)u.acc.x * u.acc.x + (double)u.acc.y * u.acc.y;
+                            zsum += 2.0 * m2;
+                            if (k2 > 0) esum += 2.0 * m2 / k2;
+                        }
+                    }
+                }
+                curr[e] = u.curr;
+            }
+            if (a.last_stage) {
+                const bool full_warps = (blockDim.x & 31) == 0;
+                if (full_warps) {
+                    if (a.flags && __any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(a.flags, FLAG_NONFINITE);
+                    if (f == 0 && a.diag) {
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            zsum += __shfl_xor_sync(0xffffffffu, zsum, o);
+                            esum += __shfl_xor_sync(0xffffffffu, esum, o);
+                        }
+                        if ((threadIdx.x & 31) == 0) { atomicAdd(&a.diag[0], zsum); atomicAdd(&a.diag[1], esum); }
+                    }
+                } else {
+                    if (a.flags && bad) atomicOr(a.flags, FLAG_NONFINITE);
+                    if (f == 0 && a.diag) { atomicAdd(&a.diag[0], zsum); atomicAdd(&a.diag[1], esum); }
+                }
+            }
+        }
+        // the buffer of the last state slab hosts the inverse transforms; the
+        // other one is free now
+        const int sx = need_acc ? sa : so;
+        if (need_old && need_acc) issue_upto(so + 4);
+        if (!a.do_inverse) { issue_upto(sx + 4); return; }
+        XchgCols<real> x{buf(sx % 3), w, TW};
+        x.sync();   // every thread has read its old/acc values
+        const int nq = f == 0 ? 4 : 2;
+        for (int qq = 0; qq < nq; ++qq) {
+            const int q = f == 0 ? (qq == 0 ? 0 : qq + 2) : (f == 1 ? (qq == 0 ? 1 : 6) : (qq == 0 ? 2 : 7));
+            cplx<real> v[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const real ky = ky_of<real>(t + TEAM * e, N, a.dky);
+                v[e] = y_mult<real>(q, curr[e], ky, kx * kx + ky * ky, sc);
+            }
+            fft.template run<true>(t, v, x);
+            cplx<real>* Y = a.Y + (size_t)q * N * H + i;
+#pragma unroll
+            for (int e = 0; e < E; ++e) Y[(size_t)(t + TEAM * e) * H] = v[e];
+            x.sync();   // the next transform reuses the buffer
+        }
+        issue_upto(sx + 4);
+    }
+
+    // a regular item: the fields fa_ (and fb_ >= 0) of tile T_
+    __device__ void item(int fa_, int fb_, int T_) {
+        fa = fa_; fb = fb_; T = T_;
+        need_old = a.mode == MODE_PROLOGUE || (a.mode == MODE_STAGE &&
+                   (a.integrator == INT_IFE || (a.integrator == INT_IFRK4 && a.stage <= 3) ||
+                    (a.integrator == INT_IFRK2 && a.stage == 1)));
+        need_acc = a.mode == MODE_STAGE && ((a.integrator == INT_IFRK4 && a.stage >= 2) ||
+                                            (a.integrator == INT_IFRK2 && a.stage == 2));
+        per_a = per_field(fa);
+        nseq = per_a + (fb >= 0 ? per_field(fb) : 0);
+        next = 0;
+        issue_upto(3);
+        field(fa, 0);
+        if (fb >= 0) field(fb, per_a);
+        __syncthreads();   // buffers free for the next item
+    }
+};
 
 // ---------------------------------------------------------------------------
 // Column kernel, edge CTA of field f: the kx = 0 and kx = N/2 columns.
@@ -225,14 +369,14 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t,
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int j = t + TEAM * e;
-                pick3(a.nl_m, f)[(size_t)j * H] = ctab[j];
+                pick3(a.nl_m, f)[(size_t)j * TW] = ctab[j];
                 pick3(a.nl_n, f)[j] = ctab[N + j];
             }
         } else if (a.mode == MODE_PROLOGUE) {
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int j = t + TEAM * e;
-                ctab[j] = om[(size_t)j * H];
+                ctab[j] = om[(size_t)j * TW];
                 ctab[N + j] = on[j];
             }
         } else {
@@ -248,7 +392,7 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t,
                 const real eyf = a.ey[cls * N + j] * a.e0[cls], eyh = a.ey[(cls + 1) * N + j] * a.e0[cls + 1];
                 // column kx = 0
                 {
-                    const size_t idx = (size_t)j * H;
+                    const size_t idx = (size_t)j * TW;   // tile 0, column 0
                     const real Ef = a.ex[cls * (H + 1)] * eyf, Eh = a.ex[(cls + 1) * (H + 1)] * eyh;
                     const cplx<real> o = need_old ? om[idx] : mk<real>(0, 0);
                     const cplx<real> ac = need_acc ? am[idx] : mk<real>(0, 0);
@@ -274,7 +418,7 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t,
                     ctab[N + j] = u.curr;
                 }
             }
-            if (a.last_stage && bad && a.flags) atomicOr(a.flags, 1u);
+            if (a.last_stage && bad && a.flags) atomicOr(a.flags, FLAG_NONFINITE);
         }
     }
     __syncthreads();
@@ -328,19 +472,35 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t,
     }
 }
 
-template <typename real, int N, int W, int E, int MINB>
-__global__ void __launch_bounds__(W * (N / E), MINB) col_kernel(const StageArgs<real> a) {
-    constexpr int H = N / 2, TILES = H / W;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx<real>* buf = reinterpret_cast<cplx<real>*>(smem_raw);
-    cplx<real>* ctab = buf + N * W;
-    const int tid = threadIdx.x, w = tid % W, t = tid / W;
-    const int blk = blockIdx.x;
-    if (blk < 3 * TILES) {
-        const int f = blk / TILES, tile = blk % TILES;
-        col_regular<real, N, W, E>(a, f, tile * W + w, t, w, buf);
-    } else {
-        col_edge<real, N, W, E>(a, blk - 3 * TILES, t, w, buf, ctab);
+template <typename real, int N, int E, int MINB>
+__global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_constant__ StageArgs<real> a) {
+    using K = ColKernel<real, N, E>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cplx<real>* bufs = reinterpret_cast<cplx<real>*>(smem_raw);
+    cplx<real>* ctab = bufs + 3 * K::SLAB;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(ctab + 2 * N);
+    int* item_sh = reinterpret_cast<int*>(mbar + 3);
+    const int tid = threadIdx.x, w = tid % TW, t = tid / TW;
+    if (tid == 0) {
+        for (int b = 0; b < 3; ++b) mbar_init(&mbar[b], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    typename K::FFT fft;
+    fft.template init<N>(t, a.tw);
+    K k{a, fft, t, w, bufs, mbar, 0u, 0, 0, 0, 0, 0, 0, false, false};
+    for (;;) {
+        if (tid == 0) *item_sh = atomicAdd(a.queue, 1);
+        __syncthreads();
+        const int item = *item_sh;
+        __syncthreads();
+        if (item >= K::NITEMS) break;
+        if (item < K::TILES) k.item(1, 2, item);
+        else if (item < 2 * K::TILES) k.item(0, -1, item - K::TILES);
+        else {
+            col_edge<real, N, TW, E>(a, item - 2 * K::TILES, t, w, bufs, ctab);
+            __syncthreads();
+        }
     }
 }
 
@@ -481,6 +641,8 @@ struct RowKernel {
         cplx<real> v[E], g0v[PH], g1v[PH];
 #pragma unroll
     for (int e = 0; e < PH; ++e) { g0v[e] = mk<real>(0, 0); g1v[e] = g0v[e]; }
+        // the column kernel that follows takes its work items from this counter
+        if (a.queue && blockIdx.x == 0 && threadIdx.x == 0) *a.queue = 0;
         fft.template init<N>(t, a.tw);
         for (int g = 0; g < NG; ++g) zero_slot0(g);
 
@@ -614,7 +776,7 @@ __global__ void __launch_bounds__(ROWS * (N / E), MINB) row_kernel(const StageAr
 
 // ---------------------------------------------------------------------------
 // Layout conversion between the reference's spectral layout (i + j*(N/2+1))
-// and the internal split layout (main[j*H + i], nyq[j]).
+// and the internal split layout (main[tidx(i, j)], nyq[j]).
 // ---------------------------------------------------------------------------
 template <typename real>
 __global__ void ref_to_internal(const cplx<real>* __restrict__ ref, cplx<real>* __restrict__ m, cplx<real>* __restrict__ nq, int N) {
@@ -622,7 +784,7 @@ __global__ void ref_to_internal(const cplx<real>* __restrict__ ref, cplx<real>* 
     const size_t total = (size_t)nxh * N;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
         const int j = (int)(k / nxh), i = (int)(k % nxh);
-        if (i < H) m[(size_t)j * H + i] = ref[k];
+        if (i < H) m[tidx(N, i, j)] = ref[k];
         else nq[j] = ref[k];
     }
 }
@@ -633,7 +795,7 @@ __global__ void internal_to_ref(const cplx<real>* __restrict__ m, const cplx<rea
     const size_t total = (size_t)nxh * N;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
         const int j = (int)(k / nxh), i = (int)(k % nxh);
-        ref[k] = (i < H) ? m[(size_t)j * H + i] : nq[j];
+        ref[k] = (i < H) ? m[tidx(N, i, j)] : nq[j];
     }
 }
 

@@ -23,17 +23,30 @@
 // that applies every multiplier in full and projects before transforming, so
 // the result equals the reference's also where the input is non-Hermitian.
 //
-// Internal layouts (N = nx = ny, H = N/2):
-//   spectral state, per field: main[j*H + i] for kx index i < H, nyq[j] for i = H
-//   Y, G arrays: [n*H + k] complex, k = x wave number (k = 0 slot unused)
+// Internal layouts (N = nx = ny, H = N/2). The state is column-tiled so that
+// TW adjacent kx columns over all N rows form one contiguous slab (one TMA
+// bulk copy):
+//   spectral state, per field: main[tidx(i, j)] for kx index i < H, nyq[j] for i = H,
+//   tidx(i, j) = (i / TW) * N * TW + j * TW + i % TW
+//   Y, G arrays: row-major [n * H + k] complex, k = x wave number (k = 0 slot
+//   unused); the column kernel fetches TW-column boxes of G with 2D TMA
 //   D (9 x N), Ed (10 x N): packed (DC + i*Nyquist) per row n
 #pragma once
 
 #include "qaf_fft.cuh"
 
+#include <cuda.h>   // CUtensorMap
+
 namespace qaf {
 
 enum StageMode : int { MODE_PROLOGUE = 0, MODE_STAGE = 1, MODE_NONL = 2 };
+
+// kx columns per tile of the column-tiled layouts (32 B of FP32 / 64 B of FP64 complex)
+constexpr int TW = 4;
+QAF_HD size_t tidx(int N, int i, int j) { return (size_t)(i / TW) * N * TW + (size_t)j * TW + (i % TW); }
+
+// status flags written by the kernels
+enum StatusFlag : unsigned { FLAG_NONFINITE = 1u, FLAG_WAIT_TIMEOUT = 2u };
 enum Integrator : int { INT_IFE = 0, INT_IFRK2 = 1, INT_IFRK4 = 2 };
 
 // physical fields produced by the row kernel's C2Rs (D slot / field id)
@@ -48,7 +61,10 @@ constexpr int NG = 7;
 constexpr int NE = 10;
 
 template <typename real>
-struct StageArgs {
+struct alignas(64) StageArgs {
+    // 2D tensor map over the G arrays viewed as [NG*N rows][H columns] of
+    // 8-byte elements (two per FP64 complex), for the column kernel's TMA boxes
+    CUtensorMap tm_G;
     // geometry and physics
     real dkx, dky;         // 2 pi / Lx, 2 pi / Ly
     real lambda;           // flow alignment
@@ -82,7 +98,8 @@ struct StageArgs {
     int mode, integrator, stage, last_stage, do_inverse;
     // diagnostics / status
     double* diag;          // [0] sum w^2 weights, [1] sum |w|^2/k^2 (half plane, Parseval weights)
-    unsigned* flags;       // bit 0: non-finite value in the new state
+    unsigned* flags;       // StatusFlag bits
+    int* queue;            // work counter of the persistent column kernel (reset by the row kernel)
     real* phys_out;        // optional: 9 physical fields + S + p11 p12 p21 (13 * N * N)
 };
 
