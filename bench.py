@@ -1,6 +1,7 @@
 """Throughput benchmark of the IF-RK4 pseudo-spectral step (w, r1, r2).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl qaf|reference] [--dtype f32|f64]
+                    [--workload plain|ensemble]
 
 Workload: the "plain throughput" configuration — 1024 x 1024 periodic grid,
 L = 16 pi, friction solver parameters Re = 1 (nu = 1), Rf = 0.1 (mu = 0.1),
@@ -23,6 +24,13 @@ Arms:
 
 Multi-GPU: the path does not shard (one grid per GPU); N GPUs run N
 independent replicas under torchrun, value = total over ranks / max time.
+
+--workload ensemble: 256 instances (seeded draw: N ~ U{64,128,256},
+activity ~ U(0.5,2), friction ~ U(0.01,0.5)), FP32, IF-RK4 dt = 1e-3, the
+other parameters as above; metric sum_i N_i^2 * steps / s. `value` is the
+batched stepper (one CUDA graph per step); `looped` is the plain solver
+looped over the same instances. Under torchrun the instances are sharded
+over ranks (strong scaling, no exchange while stepping).
 """
 from __future__ import annotations
 
@@ -44,6 +52,10 @@ L = 16 * 3.141592653589793
 DT = 5e-4
 SEED = 1
 FALLBACK_HBM_GBS = 6650.0
+ENS_COUNT = 256
+ENS_SEED = 3
+ENS_DT = 1e-3
+ENS_METRIC = "sum_i N_i^2*steps/s, 256-instance mixed-size ensemble, IF-RK4"
 
 
 def parse():
@@ -56,6 +68,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
+    ap.add_argument("--workload", choices=["plain", "ensemble"], default="plain")
+    ap.add_argument("--instances", type=int, default=ENS_COUNT)
     return ap.parse_args()
 
 
@@ -308,18 +322,192 @@ def run_reference(a, world, rank, local):
     }
 
 
+def ensemble_table(count):
+    from qaf.shard import draw_ensemble
+    return draw_ensemble(count, ENS_SEED)
+
+
+def ens_workload_desc(count):
+    return (f"ensemble of {count} instances, N ~ U{{64,128,256}}, Ra ~ U(0.5,2), Rf ~ U(0.01,0.5), FP32, "
+            f"IF-RK4 dt={ENS_DT}, L=16pi, Re=1 Er=1 lambda=0.1, draw seed {ENS_SEED}")
+
+
+def ens_cpu_baseline(sizes, steps):
+    """The FP64 host oracle on one instance of each grid size, extrapolated to the ensemble's mix."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    per = {}
+    total = 0.0
+    for n in sorted(set(sizes)):
+        p = O.params(n=n, L=L, dt=ENS_DT)
+        s0 = O.initial_spectra(SEED, n)
+        O.step(p, *s0, 1)
+        t0 = time.perf_counter()
+        O.step(p, *s0, steps)
+        per[n] = (time.perf_counter() - t0) / steps
+        total += per[n] * steps
+    work = sum(n * n for n in sizes)
+    t_step = sum(per[n] for n in sizes)
+    cores = int(os.environ.get("QAF_ORACLE_THREADS", os.cpu_count() or 1))
+    return {"value": work / t_step, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} FP64 IF-RK4 steps of one instance of each size "
+                      f"({', '.join(f'{n}^2: {per[n]*1e3:.1f} ms/step' for n in sorted(per))}; {total:.1f} s), "
+                      f"extrapolated to the ensemble's size mix with the host oracle"}
+
+
+def run_ensemble(a, world, rank, local):
+    import torch
+
+    import qaf
+    from qaf.shard import shard_instances
+
+    n_all, al_all, rf_all, seed_all = ensemble_table(a.instances)
+    mine = shard_instances(n_all, world)[rank]
+    sizes = [n_all[k] for k in mine]
+    alpha = [al_all[k] for k in mine]
+    rf = [rf_all[k] for k in mine]
+    seeds = [seed_all[k] for k in mine]
+    p = qaf.Params(re=1.0, er=1.0, rf=0.0, lam=0.1, alpha=1.0, dt=ENS_DT, q_lin=1.0, advect_omega=1)
+    ens = qaf.Ensemble(sizes, p, alpha, rf, lx=L, dtype=qaf.F32)
+    ens.init_random(seeds)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    work_mine = sum(n * n for n in sizes)
+    work_all = sum(n * n for n in n_all)
+    ngroups = len(set(sizes))
+
+    # ---- batched, device resident --------------------------------------
+    for _ in range(a.warmup):
+        ens.advance(1)
+    barrier(world)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    with ClockSampler(local) as clk:
+        barrier(world)
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record()
+            ens.advance(1)
+            e1.record()
+        barrier(world)
+    ms = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in ev), world)
+    ens.diagnostics()       # raises on a non-finite instance
+    value = work_all * a.steps / (ms * 1e-3)
+
+    # ---- the plain solver looped over the same instances ---------------
+    loop_steps = max(4, min(a.steps, 20))
+    states = []
+    for k in range(len(sizes)):
+        m = qaf.Mesh(sizes[k], lx=L, dtype=qaf.F32)
+        m.load(*m.random_q(seeds[k]))
+        states.append((m, qaf.Params(re=1.0, er=1.0, rf=rf[k], lam=0.1, alpha=alpha[k], dt=ENS_DT)))
+    for m, pk in states:
+        m.advance(pk, 2)
+    barrier(world)
+    flush.zero_()
+    l0 = torch.cuda.Event(enable_timing=True)
+    l1 = torch.cuda.Event(enable_timing=True)
+    l0.record()
+    for m, pk in states:
+        m.advance(pk, loop_steps)
+    l1.record()
+    barrier(world)
+    ms_loop = max_over_ranks(l0.elapsed_time(l1), world)
+    looped = work_all * loop_steps / (ms_loop * 1e-3)
+    del states
+
+    # ---- model bytes of one step over all instances (three-pass model) --
+    ca = lambda n: (n // 2 + 1) * n * 2 * 4
+    step_bytes = sum(4 * 55 * ca(n) for n in sizes)
+    peak, peak_kind = peaks()
+    achieved = step_bytes / (ms / a.steps * 1e-3) / 1e9
+
+    # ---- end to end: controls in, diagnostics out, every step ----------
+    for _ in range(2):
+        ens.set_controls(alpha, rf)
+        ens.advance(1)
+        ens.diagnostics()
+    barrier(world)
+    e2e_steps = max(10, a.steps // 2)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(e2e_steps)]
+    for e0, e1 in ev2:
+        flush.zero_()
+        e0.record()
+        ens.set_controls(alpha, rf)         # H2D: activity and friction factors per instance
+        ens.advance(1)
+        ens.diagnostics()                   # D2H: energy, enstrophy per instance (+ status word per size)
+        e1.record()
+    barrier(world)
+    ms2 = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in ev2), world)
+    e2e = {"value": work_all * e2e_steps / (ms2 * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": 5 * 4 * len(sizes), "d2h_bytes_per_step": 16 * len(sizes) + 4 * ngroups}
+
+    line = {
+        "metric": ENS_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded instance table; seeded random Q ~ U(-0.01,0.01), w = 0 per instance)",
+        "config": {"workload": ens_workload_desc(a.instances), "instances": a.instances,
+                   "sizes": {str(n): n_all.count(n) for n in sorted(set(n_all))},
+                   "parallelism": f"instances sharded over {world} rank(s)",
+                   "l2": "flushed (256 MiB write) between timed steps"},
+        "looped": {"value": looped, "unit": UNIT, "steps": loop_steps, "ms_per_step": ms_loop / loop_steps,
+                   "what": "the plain single-grid solver looped over this rank's instances (qaf_state_advance each)"},
+        "roofline": {"bound": "hbm", "kernel": "ensemble step (all row and column launches of every size group)",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_step": step_bytes},
+        "e2e": e2e,
+        "gpu_launches": a.steps * ngroups * 8,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = ens_cpu_baseline(n_all, a.cpu_sample_steps)
+    return line
+
+
+def run_reference_ensemble(a):
+    """The reference's CUDA build looped over the instances: one timed run per grid size, summed per instance."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness_f32")
+    if not os.path.exists(exe):
+        return {"impl": "reference", "unavailable": "the reference's CUDA build (oracle/_ref) was not built: "
+                                                    "its sources were not present when build() ran"}
+    n_all, _, _, _ = ensemble_table(a.instances)
+    per = {}
+    for n in sorted(set(n_all)):
+        cmd = [exe, "time", "--n", str(n), "--L", repr(L), "--dt", repr(ENS_DT), "--seed", str(SEED),
+               "--re", "1", "--er", "1", "--rf", "0.1", "--lambda", "0.1", "--alpha", "1",
+               "--warmup", str(a.warmup), "--timed", str(a.steps)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            return {"impl": "reference", "unavailable": f"reference build exited {r.returncode}: {r.stderr.strip()[-200:]}"}
+        per[n] = json.loads(r.stdout.strip().splitlines()[-1])["ms_per_step"]
+    ms = sum(per[n] for n in n_all)
+    work = sum(n * n for n in n_all)
+    value = work / (ms * 1e-3)
+    return {
+        "impl": "reference", "metric": ENS_METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded instance table)",
+        "config": {"workload": ens_workload_desc(a.instances), "instances": a.instances,
+                   "per_size_ms_per_step": {str(n): per[n] for n in per}},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "the reference's own CUDA build (FP32 macro shim), one timed run per grid size, "
+                                   "summed over the instances as a loop of single-grid runs"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         # one rank runs the reference; under torchrun the others exit without work
         rank, local = int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
         if rank == 0:
-            print(json.dumps(run_reference(a, 1, rank, local)), flush=True)
+            line = run_reference_ensemble(a) if a.workload == "ensemble" else run_reference(a, 1, rank, local)
+            print(json.dumps(line), flush=True)
         return
     world, rank, local = dist_init()
     import torch
     torch.cuda.set_device(local)
-    line = run_qaf(a, world, rank, local)
+    line = run_ensemble(a, world, rank, local) if a.workload == "ensemble" else run_qaf(a, world, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

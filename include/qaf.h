@@ -175,6 +175,29 @@ qaf_status qaf_init_random_q(qaf_mesh* mesh, uint64_t seed, double lo, double hi
 qaf_status qaf_diagnostics(qaf_mesh* mesh, const void* w, double* energy, double* enstrophy, double* spectrum,
                            int nshells, void* stream);
 
+/* ---- ensembles -------------------------------------------------------------
+ * No counterpart in the reference (one grid per process, friction.cu): many
+ * independent instances of mixed grid size, with their own activity Ra
+ * (alpha[k]) and friction Rf (rf[k]) and shared Re, Er, lambda, dt, q_lin,
+ * advected with IF-RK4 together. Instances of one size share each row/column
+ * launch; a step of all sizes is one CUDA graph launch (built at creation).
+ * n[k] are the grid sizes (nx = ny = n[k], see qaf_supported). */
+typedef struct qaf_ensemble qaf_ensemble;
+qaf_status qaf_ensemble_create(int ninst, const int* n, double lx, double ly, qaf_dtype dtype, const qaf_params* p,
+                               const double* alpha, const double* rf, qaf_ensemble** out);
+qaf_status qaf_ensemble_destroy(qaf_ensemble* ens);
+/* seeded random Q per instance (qaf_init_random_q with seeds[k]) */
+qaf_status qaf_ensemble_init_random(qaf_ensemble* ens, const uint64_t* seeds, double lo, double hi, void* stream);
+/* spectra of instance k in the reference layout (device pointers) */
+qaf_status qaf_ensemble_load(qaf_ensemble* ens, int k, const void* w, const void* r1, const void* r2, void* stream);
+qaf_status qaf_ensemble_store(qaf_ensemble* ens, int k, void* w, void* r1, void* r2, void* stream);
+qaf_status qaf_ensemble_advance(qaf_ensemble* ens, int nsteps, void* stream);
+/* new per-instance activity and friction (host arrays of ninst values), effective from the next
+ * step enqueued on `stream`; the values are copied before the call returns */
+qaf_status qaf_ensemble_set_controls(qaf_ensemble* ens, const double* alpha, const double* rf, void* stream);
+/* synchronises `stream`; out[2k], out[2k+1] = energy, enstrophy of instance k after the last step */
+qaf_status qaf_ensemble_diagnostics(qaf_ensemble* ens, double* out, void* stream);
+
 /* ---- allocation-free step --------------------------------------------------
  * No counterpart in the reference (whose Mesh and Field always cudaMalloc).
  * For callers that cannot allocate device memory when they step — work

@@ -9,9 +9,11 @@
 
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using namespace qaf;
@@ -161,6 +163,49 @@ Workspace<real>& ws(qaf_mesh* m);
 template <> Workspace<float>& ws<float>(qaf_mesh* m) { return m->wf; }
 template <> Workspace<double>& ws<double>(qaf_mesh* m) { return m->wd; }
 
+// twiddles exp(-2 pi i m / N), from long double
+template <typename real>
+std::vector<cplx<real>> host_twiddles(int N) {
+    std::vector<cplx<real>> tw(N);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < N; ++k) {
+        long double a = -2.0L * pi * (long double)k / (long double)N;
+        tw[k] = mk<real>((real)cosl(a), (real)sinl(a));
+    }
+    return tw;
+}
+
+// Separable integrating factors: exp(L dt) with L_w = (-kx^2 - ky^2 - Rf)/Re
+// and L_Q = -kx^2 - ky^2 + q_lin factor into exp(-c kx^2 dt) exp(-c ky^2 dt) exp(c0 dt).
+// ex/ey hold the kx/ky factors for the classes {w full, w half, Q full, Q half} step.
+template <typename real>
+void host_if_tables(int N, double dkx, double dky, double dt, double re, std::vector<real>& ex, std::vector<real>& ey) {
+    const int H = N / 2;
+    ex.assign(4 * (H + 1), 0);
+    ey.assign(4 * (size_t)N, 0);
+    const double steps[4] = {dt, 0.5 * dt, dt, 0.5 * dt};
+    const double visc[4] = {1.0 / re, 1.0 / re, 1.0, 1.0};
+    for (int c = 0; c < 4; ++c) {
+        for (int i = 0; i <= H; ++i) {
+            long double kx = (long double)dkx * i;
+            ex[c * (H + 1) + i] = (real)expl(-(long double)visc[c] * kx * kx * (long double)steps[c]);
+        }
+        for (int j = 0; j < N; ++j) {
+            long double ky = (long double)dky * (j < N / 2 + 1 ? j : j - N);
+            ey[c * N + j] = (real)expl(-(long double)visc[c] * ky * ky * (long double)steps[c]);
+        }
+    }
+}
+
+// the constant parts exp(-Rf/Re dt), exp(-Rf/Re dt/2), exp(q_lin dt), exp(q_lin dt/2)
+template <typename real>
+void host_if_e0(double dt, double re, double rf, double q_lin, real* e0) {
+    e0[0] = (real)expl(-(long double)rf / re * dt);
+    e0[1] = (real)expl(-(long double)rf / re * dt * 0.5L);
+    e0[2] = (real)expl((long double)q_lin * dt);
+    e0[3] = (real)expl((long double)q_lin * dt * 0.5L);
+}
+
 template <typename real>
 qaf_status ensure_ws(qaf_mesh* m) {
     Workspace<real>& w = ws<real>(m);
@@ -195,13 +240,7 @@ qaf_status ensure_ws(qaf_mesh* m) {
     w.diag = reinterpret_cast<double*>(b + odiag);
     w.flags = reinterpret_cast<unsigned*>(b + oflags);
     w.queue = reinterpret_cast<int*>(b + oqueue);
-    // twiddles exp(-2 pi i m / N) from long double
-    std::vector<cplx<real>> tw(N);
-    const long double pi = 3.141592653589793238462643383279502884L;
-    for (int k = 0; k < N; ++k) {
-        long double a = -2.0L * pi * (long double)k / (long double)N;
-        tw[k] = mk<real>((real)cosl(a), (real)sinl(a));
-    }
+    const std::vector<cplx<real>> tw = host_twiddles<real>(N);
     QAF_CUDA(cudaMemcpy(w.tw, tw.data(), N * sizeof(cplx<real>), cudaMemcpyHostToDevice));
     QAF_TRY(encode_g_map<real>(&w.tm_G, w.G, N));
     QAF_CUDA(cudaMemset(w.flags, 0, sizeof(unsigned)));
@@ -209,30 +248,13 @@ qaf_status ensure_ws(qaf_mesh* m) {
     return QAF_OK;
 }
 
-// Separable integrating factors: exp(L dt) with L_w = (-kx^2 - ky^2 - Rf)/Re
-// and L_Q = -kx^2 - ky^2 + q_lin factor into exp(-c kx^2 dt) exp(-c ky^2 dt) exp(c0 dt).
 template <typename real>
 qaf_status ensure_if(qaf_mesh* m, const qaf_params* p, cudaStream_t st) {
     Workspace<real>& w = ws<real>(m);
     if (w.cached[0] == p->dt && w.cached[1] == p->re && w.cached[2] == p->rf && w.cached[3] == p->q_lin) return QAF_OK;
-    const int N = m->desc.nx, H = N / 2;
-    std::vector<real> ex(4 * (H + 1)), ey(4 * N);
-    const double steps[4] = {p->dt, 0.5 * p->dt, p->dt, 0.5 * p->dt};
-    const double visc[4] = {1.0 / p->re, 1.0 / p->re, 1.0, 1.0};
-    for (int c = 0; c < 4; ++c) {
-        for (int i = 0; i <= H; ++i) {
-            long double kx = (long double)m->dkx * i;
-            ex[c * (H + 1) + i] = (real)expl(-(long double)visc[c] * kx * kx * (long double)steps[c]);
-        }
-        for (int j = 0; j < N; ++j) {
-            long double ky = (long double)m->dky * (j < N / 2 + 1 ? j : j - N);
-            ey[c * N + j] = (real)expl(-(long double)visc[c] * ky * ky * (long double)steps[c]);
-        }
-    }
-    w.e0[0] = (real)expl(-(long double)p->rf / p->re * p->dt);
-    w.e0[1] = (real)expl(-(long double)p->rf / p->re * p->dt * 0.5L);
-    w.e0[2] = (real)expl((long double)p->q_lin * p->dt);
-    w.e0[3] = (real)expl((long double)p->q_lin * p->dt * 0.5L);
+    std::vector<real> ex, ey;
+    host_if_tables<real>(m->desc.nx, m->dkx, m->dky, p->dt, p->re, ex, ey);
+    host_if_e0<real>(p->dt, p->re, p->rf, p->q_lin, w.e0);
     QAF_CUDA(cudaMemcpyAsync(w.ex, ex.data(), ex.size() * sizeof(real), cudaMemcpyHostToDevice, st));
     QAF_CUDA(cudaMemcpyAsync(w.ey, ey.data(), ey.size() * sizeof(real), cudaMemcpyHostToDevice, st));
     QAF_CUDA(cudaStreamSynchronize(st));   // host vectors go out of scope
@@ -261,6 +283,7 @@ StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
     for (int c = 0; c < 4; ++c) a.e0[c] = w.e0[c];
     a.diag = w.diag; a.flags = w.flags; a.queue = w.queue;
     a.tm_G = w.tm_G;
+    a.ninst = 1;
     return a;
 }
 
@@ -270,7 +293,7 @@ StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
 template <typename real, int N>
 struct Launch {
     using C = Cfg<real, N>;
-    static inline int col_blocks = 0;   // persistent grid: resident CTAs, at most the item count
+    static inline int col_slots = 0;    // resident column CTAs on the device (persistent grid size)
     static qaf_status setup() {
         static bool done = false;
         if (done) return QAF_OK;
@@ -284,15 +307,17 @@ struct Launch {
         QAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_kernel<real, N, C::EC, C::MINB>,
                                                                C::COL_THREADS, C::COL_SMEM));
         if (per_sm < 1) return fail(QAF_ERR_UNSUPPORTED, "column kernel does not fit on an SM");
-        col_blocks = sms * per_sm < C::COL_ITEMS ? sms * per_sm : C::COL_ITEMS;
+        col_slots = sms * per_sm;
         done = true;
         return QAF_OK;
     }
     static void col(const StageArgs<real>& a, cudaStream_t st) {
-        col_kernel<real, N, C::EC, C::MINB><<<col_blocks, C::COL_THREADS, C::COL_SMEM, st>>>(a);
+        const long items = (long)C::COL_ITEMS * a.ninst;
+        const int grid = items < col_slots ? (int)items : col_slots;
+        col_kernel<real, N, C::EC, C::MINB><<<grid, C::COL_THREADS, C::COL_SMEM, st>>>(a);
     }
     static void row(const StageArgs<real>& a, cudaStream_t st) {
-        row_kernel<real, N, C::ER, C::ROWS, C::MINB><<<C::ROW_BLOCKS, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
+        row_kernel<real, N, C::ER, C::ROWS, C::MINB><<<C::ROW_BLOCKS * a.ninst, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
     }
     static void bwd(const cplx<real>* spec, cplx<real>* T, real* phys, const cplx<real>* tw, cudaStream_t st) {
         col_ifft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COLT_THREADS, C::COLT_SMEM, st>>>(spec, T, tw);
@@ -1046,3 +1071,459 @@ extern "C" qaf_status qaf_step_noalloc(int n, double lx, double ly, qaf_dtype dt
     void* st[3] = {w, r1, r2};
     return dispatch<OpStepNoAlloc>(&m, &m, scratch, p, (int)integ, (void* const*)st, nsteps, (cudaStream_t)stream);
 }
+
+// ===========================================================================
+// Ensembles: many independent instances of mixed grid size and parameters,
+// advanced together. Instances of one grid size form a group whose buffers
+// share one allocation with a fixed per-instance stride, so each row or
+// column launch serves the whole group (the row grid spans every instance's
+// rows, the persistent column kernel's queue every instance's tiles). One
+// step of all groups is captured once into a CUDA graph, the groups as
+// parallel branches, and replayed per step.
+// ===========================================================================
+namespace {
+
+template <typename real>
+struct EnsGroup {
+    int N = 0, ninst = 0;
+    std::vector<int> members;       // ensemble instance ids in group order
+    size_t istride = 0;             // complex elements per instance
+    cplx<real>* block = nullptr;    // ninst * istride: per-instance buffers
+    void* shared = nullptr;         // tables, per-instance parameters, diagnostics, status
+    Workspace<real> w;              // instance-0 pointers and the shared tables
+    real* inst_alpha = nullptr;
+    real* inst_e0 = nullptr;
+    double* diag = nullptr;         // 2 per instance
+};
+
+// per-instance buffer layout (complex elements), returned size rounded up to
+// a multiple of H so that instance k's G rows start at row k*istride/H
+template <typename real>
+size_t carve_instance(Workspace<real>& w, cplx<real>* b, int N) {
+    const int H = N / 2;
+    const size_t plane = (size_t)N * H;
+    size_t off = 0;
+    auto take = [&](size_t n) { size_t o = off; off += align_up(n); return o; };
+    for (int f = 0; f < 3; ++f) { w.old_m[f] = b + take(plane); w.old_n[f] = b + take(N); }
+    for (int f = 0; f < 3; ++f) { w.acc_m[f] = b + take(plane); w.acc_n[f] = b + take(N); }
+    w.Y = b + take(NY * plane);
+    w.D = b + take((size_t)PF_COUNT * N);
+    w.G = b + take(NG * plane);
+    w.Ed = b + take((size_t)NE * N);
+    const size_t unit = (size_t)H > 32 ? (size_t)H : 32;
+    return (off + unit - 1) / unit * unit;
+}
+
+}  // namespace
+
+struct qaf_ensemble {
+    qaf_dtype dtype;
+    double lx, ly;
+    qaf_params p;
+    int ninst;
+    std::vector<int> n_of;
+    std::vector<std::pair<int, int>> where;   // instance -> (group, slot)
+    std::vector<EnsGroup<float>> gf;
+    std::vector<EnsGroup<double>> gd;
+    bool y_valid = false;
+    cudaStream_t cap = nullptr;
+    std::vector<cudaStream_t> gstream;
+    std::vector<cudaEvent_t> gevent;
+    cudaEvent_t fork = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void* staging = nullptr;          // pinned host copy of the per-instance controls
+    size_t staging_bytes = 0;
+    cudaEvent_t staged = nullptr;     // the last upload from `staging` has been read
+};
+
+namespace {
+
+template <typename real> std::vector<EnsGroup<real>>& groups(qaf_ensemble* e);
+template <> std::vector<EnsGroup<float>>& groups<float>(qaf_ensemble* e) { return e->gf; }
+template <> std::vector<EnsGroup<double>>& groups<double>(qaf_ensemble* e) { return e->gd; }
+
+// call f(std::integral_constant<int, N>) for a supported N
+template <class F>
+qaf_status with_n(int N, F&& f) {
+    switch (N) {
+        case 16: return f(std::integral_constant<int, 16>{});
+        case 32: return f(std::integral_constant<int, 32>{});
+        case 64: return f(std::integral_constant<int, 64>{});
+        case 128: return f(std::integral_constant<int, 128>{});
+        case 256: return f(std::integral_constant<int, 256>{});
+        case 512: return f(std::integral_constant<int, 512>{});
+        case 1024: return f(std::integral_constant<int, 1024>{});
+        default: return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size");
+    }
+}
+
+template <typename real>
+StageArgs<real> group_args(const qaf_ensemble* e, const EnsGroup<real>& g) {
+    StageArgs<real> a;
+    std::memset(&a, 0, sizeof(a));
+    const int N = g.N, nxh = N / 2 + 1;
+    a.dkx = (real)(2 * M_PI / e->lx); a.dky = (real)(2 * M_PI / e->ly);
+    a.lambda = (real)e->p.lambda; a.ce = (real)(1.0 / (e->p.er * e->p.re)); a.alpha = (real)e->p.alpha;
+    a.dt = (real)e->p.dt; a.advect = e->p.advect_omega ? 1 : 0;
+    a.kx_keep = (nxh - 1) * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
+    for (int f = 0; f < 3; ++f) {
+        a.old_m[f] = g.w.old_m[f]; a.old_n[f] = g.w.old_n[f]; a.acc_m[f] = g.w.acc_m[f]; a.acc_n[f] = g.w.acc_n[f];
+        a.nl_m[f] = g.w.acc_m[f]; a.nl_n[f] = g.w.acc_n[f];
+    }
+    a.Y = g.w.Y; a.D = g.w.D; a.G = g.w.G; a.Ed = g.w.Ed; a.tw = g.w.tw; a.ex = g.w.ex; a.ey = g.w.ey;
+    a.flags = g.w.flags; a.queue = g.w.queue; a.tm_G = g.w.tm_G;
+    a.ninst = g.ninst; a.istride = g.istride;
+    a.inst_alpha = g.inst_alpha; a.inst_e0 = g.inst_e0;
+    a.diag = g.diag; a.diag_istride = 2;
+    a.integrator = INT_IFRK4;
+    return a;
+}
+
+template <typename real>
+qaf_status build_groups(qaf_ensemble* e, const double* alpha, const double* rf) {
+    auto& G = groups<real>(e);
+    std::vector<int> sizes(e->n_of);
+    std::sort(sizes.begin(), sizes.end());
+    sizes.erase(std::unique(sizes.begin(), sizes.end()), sizes.end());
+    e->where.assign(e->ninst, {-1, -1});
+    for (int N : sizes) {
+        EnsGroup<real> g;
+        g.N = N;
+        for (int k = 0; k < e->ninst; ++k)
+            if (e->n_of[k] == N) { e->where[k] = {(int)G.size(), (int)g.members.size()}; g.members.push_back(k); }
+        g.ninst = (int)g.members.size();
+        Workspace<real> probe;
+        g.istride = carve_instance<real>(probe, nullptr, N);
+        cplx<real>* blk = nullptr;
+        cudaError_t er = cudaMalloc((void**)&blk, g.istride * g.ninst * sizeof(cplx<real>));
+        if (er != cudaSuccess) return fail(QAF_ERR_ALLOC, std::string("ensemble cudaMalloc: ") + cudaGetErrorString(er));
+        g.block = blk;
+        carve_instance<real>(g.w, blk, N);
+        // shared: tw (N), ex (4(H+1)), ey (4N), alpha (ninst), e0 (4 ninst), diag (2 ninst), flags, queue
+        const int H = N / 2;
+        const size_t bytes = N * sizeof(cplx<real>) + (4 * (H + 1) + 4 * N + 5 * (size_t)g.ninst) * sizeof(real) +
+                             2 * (size_t)g.ninst * sizeof(double) + 256;
+        void* sh = nullptr;
+        er = cudaMalloc(&sh, bytes);
+        if (er != cudaSuccess) return fail(QAF_ERR_ALLOC, std::string("ensemble cudaMalloc: ") + cudaGetErrorString(er));
+        g.shared = sh;
+        char* c = static_cast<char*>(sh);
+        g.diag = reinterpret_cast<double*>(c); c += 2 * (size_t)g.ninst * sizeof(double);
+        g.w.tw = reinterpret_cast<cplx<real>*>(c); c += N * sizeof(cplx<real>);
+        g.w.ex = reinterpret_cast<real*>(c); c += 4 * (H + 1) * sizeof(real);
+        g.w.ey = reinterpret_cast<real*>(c); c += 4 * (size_t)N * sizeof(real);
+        g.inst_alpha = reinterpret_cast<real*>(c); c += g.ninst * sizeof(real);
+        g.inst_e0 = reinterpret_cast<real*>(c); c += 4 * (size_t)g.ninst * sizeof(real);
+        c = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(c) + 15) & ~uintptr_t(15));
+        g.w.flags = reinterpret_cast<unsigned*>(c); c += 16;
+        g.w.queue = reinterpret_cast<int*>(c);
+        // host-built tables, the same as a single mesh's
+        const std::vector<cplx<real>> tw = host_twiddles<real>(N);
+        std::vector<real> ex, ey, ia(g.ninst), ie0(4 * (size_t)g.ninst);
+        host_if_tables<real>(N, 2 * M_PI / e->lx, 2 * M_PI / e->ly, e->p.dt, e->p.re, ex, ey);
+        for (int s2 = 0; s2 < g.ninst; ++s2) {
+            const int k = g.members[s2];
+            ia[s2] = (real)alpha[k];
+            host_if_e0<real>(e->p.dt, e->p.re, rf[k], e->p.q_lin, &ie0[4 * (size_t)s2]);
+        }
+        QAF_CUDA(cudaMemcpy(g.w.tw, tw.data(), tw.size() * sizeof(cplx<real>), cudaMemcpyHostToDevice));
+        QAF_CUDA(cudaMemcpy(g.w.ex, ex.data(), ex.size() * sizeof(real), cudaMemcpyHostToDevice));
+        QAF_CUDA(cudaMemcpy(g.w.ey, ey.data(), ey.size() * sizeof(real), cudaMemcpyHostToDevice));
+        QAF_CUDA(cudaMemcpy(g.inst_alpha, ia.data(), ia.size() * sizeof(real), cudaMemcpyHostToDevice));
+        QAF_CUDA(cudaMemcpy(g.inst_e0, ie0.data(), ie0.size() * sizeof(real), cudaMemcpyHostToDevice));
+        QAF_CUDA(cudaMemset(g.w.flags, 0, 16));
+        QAF_CUDA(cudaMemset(g.diag, 0, 2 * (size_t)g.ninst * sizeof(double)));
+        // TMA view of every instance's G arrays
+        {
+            static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+            if (!encode) {
+                cudaDriverEntryPointQueryResult q;
+                void* fn = nullptr;
+                QAF_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+                if (q != cudaDriverEntryPointSuccess || !fn) return fail(QAF_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+                encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+            }
+            const cuuint64_t cpe = sizeof(cplx<real>) / 8;
+            cuuint64_t dims[2] = {(cuuint64_t)H * cpe, (cuuint64_t)(g.ninst - 1) * (g.istride / H) + (cuuint64_t)NG * N};
+            cuuint64_t strides[1] = {(cuuint64_t)H * cpe * 8};
+            cuuint32_t box[2] = {(cuuint32_t)(TW * cpe), (cuuint32_t)(N < 256 ? N : 256)};
+            cuuint32_t estr[2] = {1, 1};
+            CUresult r = encode(&g.w.tm_G, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, g.w.G, dims, strides, box, estr,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return fail(QAF_ERR_CUDA, "cuTensorMapEncodeTiled failed (ensemble)");
+        }
+        qaf_status st = with_n(N, [&](auto n) -> qaf_status { return Launch<real, decltype(n)::value>::setup(); });
+        if (st != QAF_OK) return st;
+        G.push_back(g);
+    }
+    return QAF_OK;
+}
+
+template <typename real>
+qaf_status ens_prologue(qaf_ensemble* e, cudaStream_t st) {
+    for (auto& g : groups<real>(e)) {
+        StageArgs<real> a = group_args<real>(e, g);
+        a.mode = MODE_PROLOGUE;
+        a.do_inverse = 1;
+        QAF_CUDA(cudaMemsetAsync(g.w.queue, 0, sizeof(int), st));
+        qaf_status s2 = with_n(g.N, [&](auto n) -> qaf_status {
+            Launch<real, decltype(n)::value>::col(a, st);
+            return QAF_OK;
+        });
+        if (s2 != QAF_OK) return s2;
+    }
+    return post_launch("ensemble prologue");
+}
+
+// one IF-RK4 step of every group, each group on its own stream
+template <typename real>
+qaf_status ens_capture(qaf_ensemble* e) {
+    auto& G = groups<real>(e);
+    QAF_CUDA(cudaStreamBeginCapture(e->cap, cudaStreamCaptureModeThreadLocal));
+    QAF_CUDA(cudaEventRecord(e->fork, e->cap));
+    for (size_t gi = 0; gi < G.size(); ++gi) {
+        auto& g = G[gi];
+        cudaStream_t st = e->gstream[gi];
+        QAF_CUDA(cudaStreamWaitEvent(st, e->fork, 0));
+        QAF_CUDA(cudaMemsetAsync(g.diag, 0, 2 * (size_t)g.ninst * sizeof(double), st));
+        StageArgs<real> a = group_args<real>(e, g);
+        a.mode = MODE_STAGE;
+        a.do_inverse = 1;
+        qaf_status s2 = with_n(g.N, [&](auto n) -> qaf_status {
+            for (int k = 1; k <= 4; ++k) {
+                a.stage = k;
+                a.last_stage = k == 4;
+                Launch<real, decltype(n)::value>::row(a, st);
+                Launch<real, decltype(n)::value>::col(a, st);
+            }
+            return QAF_OK;
+        });
+        if (s2 != QAF_OK) return s2;
+        QAF_CUDA(cudaEventRecord(e->gevent[gi], st));
+        QAF_CUDA(cudaStreamWaitEvent(e->cap, e->gevent[gi], 0));
+    }
+    QAF_CUDA(cudaStreamEndCapture(e->cap, &e->graph));
+    QAF_CUDA(cudaGraphInstantiate(&e->exec, e->graph, 0));
+    return QAF_OK;
+}
+
+qaf_status check_ens(const qaf_ensemble* e, int inst) {
+    if (!e) return fail(QAF_ERR_INVALID, "null ensemble");
+    if (inst < 0 || inst >= e->ninst) return fail(QAF_ERR_INVALID, "instance index out of range");
+    return QAF_OK;
+}
+
+template <typename real>
+qaf_status ens_copy(qaf_ensemble* e, int inst, void* const* st3, bool load, cudaStream_t st) {
+    auto& g = groups<real>(e)[e->where[inst].first];
+    const size_t io = (size_t)e->where[inst].second * g.istride;
+    const size_t n = (size_t)(g.N / 2 + 1) * g.N;
+    for (int f = 0; f < 3; ++f) {
+        if (load)
+            ref_to_internal<real><<<grid_for(n), 256, 0, st>>>(reinterpret_cast<const cplx<real>*>(st3[f]),
+                                                             g.w.old_m[f] + io, g.w.old_n[f] + io, g.N);
+        else
+            internal_to_ref<real><<<grid_for(n), 256, 0, st>>>(g.w.old_m[f] + io, g.w.old_n[f] + io,
+                                                             reinterpret_cast<cplx<real>*>(st3[f]), g.N);
+    }
+    if (load) e->y_valid = false;
+    return post_launch(load ? "qaf_ensemble_load" : "qaf_ensemble_store");
+}
+
+// per-instance alpha and e0 of every group, packed group after group
+template <typename real>
+qaf_status ens_controls(qaf_ensemble* e, const double* alpha, const double* rf, cudaStream_t st) {
+    auto& G = groups<real>(e);
+    size_t need = 0;
+    for (auto& g : G) need += 5 * (size_t)g.ninst * sizeof(real);
+    if (!e->staging) {
+        QAF_CUDA(cudaMallocHost(&e->staging, need));
+        e->staging_bytes = need;
+        QAF_CUDA(cudaEventCreateWithFlags(&e->staged, cudaEventDisableTiming));
+    } else {
+        QAF_CUDA(cudaEventSynchronize(e->staged));   // the previous upload has left the buffer
+    }
+    real* h = static_cast<real*>(e->staging);
+    for (auto& g : G) {
+        real* ha = h;
+        real* he = h + g.ninst;
+        for (int s2 = 0; s2 < g.ninst; ++s2) {
+            const int k = g.members[s2];
+            ha[s2] = (real)alpha[k];
+            host_if_e0<real>(e->p.dt, e->p.re, rf[k], e->p.q_lin, he + 4 * (size_t)s2);
+        }
+        QAF_CUDA(cudaMemcpyAsync(g.inst_alpha, ha, g.ninst * sizeof(real), cudaMemcpyHostToDevice, st));
+        QAF_CUDA(cudaMemcpyAsync(g.inst_e0, he, 4 * (size_t)g.ninst * sizeof(real), cudaMemcpyHostToDevice, st));
+        h += 5 * (size_t)g.ninst;
+    }
+    QAF_CUDA(cudaEventRecord(e->staged, st));
+    return QAF_OK;
+}
+
+template <typename real>
+void ens_free(qaf_ensemble* e) {
+    for (auto& g : groups<real>(e)) {
+        if (g.block) cudaFree(g.block);
+        if (g.shared) cudaFree(g.shared);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+qaf_status qaf_ensemble_create(int ninst, const int* n, double lx, double ly, qaf_dtype dtype, const qaf_params* p,
+                               const double* alpha, const double* rf, qaf_ensemble** out) {
+    if (!out || !n || !p || !alpha || !rf) return fail(QAF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (ninst < 1) return fail(QAF_ERR_INVALID, "need at least one instance");
+    if (!(lx > 0) || !(ly > 0)) return fail(QAF_ERR_INVALID, "lx, ly must be positive");
+    if (dtype != QAF_F32 && dtype != QAF_F64) return fail(QAF_ERR_INVALID, "bad dtype");
+    QAF_TRY(check_params(p));
+    for (int k = 0; k < ninst; ++k) {
+        if (!qaf_supported(n[k], dtype)) return fail(QAF_ERR_UNSUPPORTED, "an instance grid size has no kernels");
+        if (!std::isfinite(alpha[k]) || !std::isfinite(rf[k])) return fail(QAF_ERR_INVALID, "non-finite alpha or rf");
+    }
+    qaf_ensemble* e = new qaf_ensemble();
+    e->dtype = dtype; e->lx = lx; e->ly = ly; e->p = *p; e->p.alpha_field = nullptr; e->ninst = ninst;
+    e->n_of.assign(n, n + ninst);
+    qaf_status s = dtype == QAF_F64 ? build_groups<double>(e, alpha, rf) : build_groups<float>(e, alpha, rf);
+    const size_t ng = dtype == QAF_F64 ? e->gd.size() : e->gf.size();
+    if (s == QAF_OK) {
+        cudaError_t er = cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking);
+        if (er == cudaSuccess) er = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+        for (size_t gi = 0; gi < ng && er == cudaSuccess; ++gi) {
+            cudaStream_t st;
+            cudaEvent_t ev;
+            er = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+            if (er == cudaSuccess) { e->gstream.push_back(st); er = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming); }
+            if (er == cudaSuccess) e->gevent.push_back(ev);
+        }
+        if (er != cudaSuccess) s = fail(QAF_ERR_CUDA, std::string("ensemble streams: ") + cudaGetErrorString(er));
+    }
+    if (s == QAF_OK) s = dtype == QAF_F64 ? ens_capture<double>(e) : ens_capture<float>(e);
+    if (s != QAF_OK) {
+        qaf_ensemble_destroy(e);
+        return s;
+    }
+    *out = e;
+    return QAF_OK;
+}
+
+qaf_status qaf_ensemble_destroy(qaf_ensemble* e) {
+    if (!e) return QAF_OK;
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    for (cudaStream_t st : e->gstream) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : e->gevent) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->cap) cudaStreamDestroy(e->cap);
+    if (e->staged) { cudaEventSynchronize(e->staged); cudaEventDestroy(e->staged); }
+    if (e->staging) cudaFreeHost(e->staging);
+    if (e->dtype == QAF_F64) ens_free<double>(e); else ens_free<float>(e);
+    delete e;
+    return QAF_OK;
+}
+
+qaf_status qaf_ensemble_load(qaf_ensemble* e, int inst, const void* w, const void* r1, const void* r2, void* stream) {
+    QAF_TRY(check_ens(e, inst));
+    if (!w || !r1 || !r2) return fail(QAF_ERR_INVALID, "null pointer");
+    void* st3[3] = {const_cast<void*>(w), const_cast<void*>(r1), const_cast<void*>(r2)};
+    return e->dtype == QAF_F64 ? ens_copy<double>(e, inst, st3, true, (cudaStream_t)stream)
+                               : ens_copy<float>(e, inst, st3, true, (cudaStream_t)stream);
+}
+
+qaf_status qaf_ensemble_store(qaf_ensemble* e, int inst, void* w, void* r1, void* r2, void* stream) {
+    QAF_TRY(check_ens(e, inst));
+    if (!w || !r1 || !r2) return fail(QAF_ERR_INVALID, "null pointer");
+    void* st3[3] = {w, r1, r2};
+    return e->dtype == QAF_F64 ? ens_copy<double>(e, inst, st3, false, (cudaStream_t)stream)
+                               : ens_copy<float>(e, inst, st3, false, (cudaStream_t)stream);
+}
+
+qaf_status qaf_ensemble_advance(qaf_ensemble* e, int nsteps, void* stream) {
+    QAF_TRY(check_ens(e, 0));
+    if (nsteps < 0) return fail(QAF_ERR_INVALID, "nsteps < 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!e->y_valid) {
+        QAF_TRY(e->dtype == QAF_F64 ? ens_prologue<double>(e, st) : ens_prologue<float>(e, st));
+        e->y_valid = true;
+    }
+    for (int s = 0; s < nsteps; ++s) QAF_CUDA(cudaGraphLaunch(e->exec, st));
+    return QAF_OK;
+}
+
+qaf_status qaf_ensemble_set_controls(qaf_ensemble* e, const double* alpha, const double* rf, void* stream) {
+    QAF_TRY(check_ens(e, 0));
+    if (!alpha || !rf) return fail(QAF_ERR_INVALID, "null pointer");
+    for (int k = 0; k < e->ninst; ++k)
+        if (!std::isfinite(alpha[k]) || !std::isfinite(rf[k])) return fail(QAF_ERR_INVALID, "non-finite alpha or rf");
+    return e->dtype == QAF_F64 ? ens_controls<double>(e, alpha, rf, (cudaStream_t)stream)
+                               : ens_controls<float>(e, alpha, rf, (cudaStream_t)stream);
+}
+
+qaf_status qaf_ensemble_diagnostics(qaf_ensemble* e, double* out, void* stream) {
+    QAF_TRY(check_ens(e, 0));
+    if (!out) return fail(QAF_ERR_INVALID, "null pointer");
+    QAF_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    unsigned flags = 0;
+    auto gather = [&](auto& G) -> qaf_status {
+        for (auto& g : G) {
+            std::vector<double> h(2 * (size_t)g.ninst);
+            unsigned fl = 0;
+            QAF_CUDA(cudaMemcpy(h.data(), g.diag, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            QAF_CUDA(cudaMemcpy(&fl, g.w.flags, sizeof(fl), cudaMemcpyDeviceToHost));
+            flags |= fl;
+            const double n4 = (double)g.N * g.N * (double)g.N * g.N;
+            for (int s2 = 0; s2 < g.ninst; ++s2) {
+                out[2 * g.members[s2] + 0] = 0.5 * h[2 * s2 + 1] / n4;
+                out[2 * g.members[s2] + 1] = 0.5 * h[2 * s2 + 0] / n4;
+            }
+        }
+        return QAF_OK;
+    };
+    QAF_TRY(e->dtype == QAF_F64 ? gather(e->gd) : gather(e->gf));
+    if (flags & FLAG_WAIT_TIMEOUT) return fail(QAF_ERR_CUDA, "a kernel's wait for its own copy timed out");
+    if (flags) return fail(QAF_ERR_NONFINITE, "an instance produced a non-finite value");
+    return QAF_OK;
+}
+
+qaf_status qaf_ensemble_init_random(qaf_ensemble* e, const uint64_t* seeds, double lo, double hi, void* stream) {
+    QAF_TRY(check_ens(e, 0));
+    if (!seeds) return fail(QAF_ERR_INVALID, "null seeds");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t rb = e->dtype == QAF_F64 ? 8 : 4;
+    const int nmax = *std::max_element(e->n_of.begin(), e->n_of.end());
+    const size_t smax = (size_t)(nmax / 2 + 1) * nmax * 2 * rb;
+    void* buf = nullptr;
+    if (cudaMalloc(&buf, 3 * smax) != cudaSuccess) return fail(QAF_ERR_ALLOC, "ensemble init cudaMalloc");
+    char* b = static_cast<char*>(buf);
+    std::vector<std::pair<int, qaf_mesh*>> meshes;   // one transform mesh per grid size
+    qaf_status s = QAF_OK;
+    for (int k = 0; k < e->ninst && s == QAF_OK; ++k) {
+        const int N = e->n_of[k];
+        const size_t sb = (size_t)(N / 2 + 1) * N * 2 * rb;
+        qaf_mesh* m = nullptr;
+        for (auto& pm : meshes)
+            if (pm.first == N) m = pm.second;
+        if (!m) {
+            qaf_mesh_desc d{N, N, e->lx, e->ly, e->dtype};
+            s = qaf_mesh_create(&d, &m);
+            if (s != QAF_OK) break;
+            meshes.push_back({N, m});
+        }
+        s = qaf_init_random_q(m, seeds[k], lo, hi, b, b + sb, b + 2 * sb, stream);
+        if (s == QAF_OK) s = qaf_ensemble_load(e, k, b, b + sb, b + 2 * sb, stream);
+    }
+    if (s == QAF_OK) {
+        cudaError_t er = cudaStreamSynchronize(st);
+        if (er != cudaSuccess) s = fail(QAF_ERR_CUDA, cudaGetErrorString(er));
+    }
+    cudaFree(buf);
+    for (auto& pm : meshes) qaf_mesh_destroy(pm.second);
+    return s;
+}
+
+}  // extern "C"

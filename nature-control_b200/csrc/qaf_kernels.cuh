@@ -88,6 +88,8 @@ struct ColKernel {
     // its G arrays (none in the prologue), then old and/or acc
     int fa, fb, T, nseq, next, per_a;
     bool need_old, need_acc;
+    int inst;              // instance of the current item
+    size_t io;             // its buffer offset (complex elements)
 
     __device__ cplx<real>* buf(int b) const { return bufs + (size_t)b * SLAB; }
     __device__ int nG(int f) const { return a.mode == MODE_PROLOGUE ? 0 : (f == 0 ? 3 : 2); }
@@ -101,7 +103,7 @@ struct ColKernel {
     __device__ const cplx<real>* slab_state(int sidx) const {
         const int f = sidx < per_a ? fa : fb;
         const int r = sidx < per_a ? sidx : sidx - per_a;
-        const size_t base = (size_t)T * SLAB;
+        const size_t base = io + (size_t)T * SLAB;
         if (r == nG(f) && need_old) return pick3(a.old_m, f) + base;
         return pick3(a.acc_m, f) + base;
     }
@@ -121,7 +123,8 @@ struct ColKernel {
                     constexpr int CPE = sizeof(cplx<real>) / 8;   // 8-byte elements per complex
 #pragma unroll 1
                     for (int r0 = 0; r0 < N; r0 += BOXR)
-                        tile_load_2d(buf(b) + (size_t)r0 * TW, &a.tm_G, T * TW * CPE, g * N + r0, &mbar[b]);
+                        tile_load_2d(buf(b) + (size_t)r0 * TW, &a.tm_G, T * TW * CPE,
+                                     (int)((io / H) + (size_t)g * N + r0), &mbar[b]);
                 } else {
                     bulk_load(buf(b), slab_state(next), bytes, &mbar[b]);
                 }
@@ -161,7 +164,7 @@ struct ColKernel {
         const real kx = a.dkx * (real)i;
         const real sc = (real)1 / ((real)N * (real)N);
         const int ng = nG(f);
-        const size_t base = (size_t)T * SLAB;
+        const size_t base = io + (size_t)T * SLAB;
         cplx<real> nl[E], curr[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) nl[e] = mk<real>(0, 0);
@@ -187,8 +190,9 @@ struct ColKernel {
             for (int e = 0; e < E; ++e) curr[e] = ob[(t + TEAM * e) * TW + w];
         } else {
             const int cls = f == 0 ? 0 : 2;
-            const real exf = a.ex[cls * (H + 1) + i] * a.e0[cls];
-            const real exh = a.ex[(cls + 1) * (H + 1) + i] * a.e0[cls + 1];
+            const real* e0 = a.inst_e0 ? a.inst_e0 + 4 * inst : a.e0;
+            const real exf = a.ex[cls * (H + 1) + i] * e0[cls];
+            const real exh = a.ex[(cls + 1) * (H + 1) + i] * e0[cls + 1];
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int j = t + TEAM * e;
@@ -224,11 +228,17 @@ struct ColKernel {
                             zsum += __shfl_xor_sync(0xffffffffu, zsum, o);
                             esum += __shfl_xor_sync(0xffffffffu, esum, o);
                         }
-                        if ((threadIdx.x & 31) == 0) { atomicAdd(&a.diag[0], zsum); atomicAdd(&a.diag[1], esum); }
+                        if ((threadIdx.x & 31) == 0) {
+                            double* dg = a.diag + a.diag_istride * inst;
+                            atomicAdd(&dg[0], zsum); atomicAdd(&dg[1], esum);
+                        }
                     }
                 } else {
                     if (a.flags && bad) atomicOr(a.flags, FLAG_NONFINITE);
-                    if (f == 0 && a.diag) { atomicAdd(&a.diag[0], zsum); atomicAdd(&a.diag[1], esum); }
+                    if (f == 0 && a.diag) {
+                        double* dg = a.diag + a.diag_istride * inst;
+                        atomicAdd(&dg[0], zsum); atomicAdd(&dg[1], esum);
+                    }
                 }
             }
         }
@@ -249,7 +259,7 @@ struct ColKernel {
                 v[e] = y_mult<real>(q, curr[e], ky, kx * kx + ky * ky, sc);
             }
             fft.template run<true>(t, v, x);
-            cplx<real>* Y = a.Y + (size_t)q * N * H + i;
+            cplx<real>* Y = a.Y + io + (size_t)q * N * H + i;
 #pragma unroll
             for (int e = 0; e < E; ++e) Y[(size_t)(t + TEAM * e) * H] = v[e];
             x.sync();   // the next transform reuses the buffer
@@ -257,9 +267,11 @@ struct ColKernel {
         issue_upto(sx + 4);
     }
 
-    // a regular item: the fields fa_ (and fb_ >= 0) of tile T_
-    __device__ void item(int fa_, int fb_, int T_) {
+    // a regular item: the fields fa_ (and fb_ >= 0) of tile T_ of instance inst_
+    __device__ void item(int fa_, int fb_, int T_, int inst_) {
         fa = fa_; fb = fb_; T = T_;
+        inst = inst_;
+        io = (size_t)inst_ * a.istride;
         need_old = a.mode == MODE_PROLOGUE || (a.mode == MODE_STAGE &&
                    (a.integrator == INT_IFE || (a.integrator == INT_IFRK4 && a.stage <= 3) ||
                     (a.integrator == INT_IFRK2 && a.stage == 1)));
@@ -300,8 +312,9 @@ __device__ __forceinline__ void edge_product_mults(int p, real ky, real kN, real
 }
 
 template <typename real, int N, int W, int E>
-__device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t, int w, cplx<real>* buf,
+__device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int inst, int t, int w, cplx<real>* buf,
                                          cplx<real>* ctab) {
+    const size_t io = (size_t)inst * a.istride;
     constexpr int H = N / 2, TEAM = N / E;
     XchgCols<real> x{buf, w, W};
     TeamFFT<real, N, E> fft;
@@ -323,7 +336,7 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t,
             const bool active = base + w < np;
             const int p = pbase + (active ? base + w : 0);
 #pragma unroll
-            for (int e = 0; e < E; ++e) v[e] = active ? a.Ed[(size_t)p * N + t + TEAM * e] : mk<real>(0, 0);
+            for (int e = 0; e < E; ++e) v[e] = active ? a.Ed[io + (size_t)p * N + t + TEAM * e] : mk<real>(0, 0);
             fft.template run<false>(t, v, x);
             // unpack the two real sequences: DC = (Z[j] + conj Z[-j]) / 2, NYQ = (Z[j] - conj Z[-j]) / 2i
             cplx<real> zm[E];
@@ -361,16 +374,16 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t,
     }
 
     if (w == 0) {
-        cplx<real>* om = pick3(a.old_m, f);
-        cplx<real>* on = pick3(a.old_n, f);
-        cplx<real>* am = pick3(a.acc_m, f);
-        cplx<real>* an = pick3(a.acc_n, f);
+        cplx<real>* om = pick3(a.old_m, f) + io;
+        cplx<real>* on = pick3(a.old_n, f) + io;
+        cplx<real>* am = pick3(a.acc_m, f) + io;
+        cplx<real>* an = pick3(a.acc_n, f) + io;
         if (a.mode == MODE_NONL) {
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int j = t + TEAM * e;
-                pick3(a.nl_m, f)[(size_t)j * TW] = ctab[j];
-                pick3(a.nl_n, f)[j] = ctab[N + j];
+                pick3(a.nl_m, f)[io + (size_t)j * TW] = ctab[j];
+                pick3(a.nl_n, f)[io + j] = ctab[N + j];
             }
         } else if (a.mode == MODE_PROLOGUE) {
 #pragma unroll
@@ -389,7 +402,8 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t,
             for (int e = 0; e < E; ++e) {
                 const int j = t + TEAM * e;
                 const real ky = ky_of<real>(j, N, a.dky);
-                const real eyf = a.ey[cls * N + j] * a.e0[cls], eyh = a.ey[(cls + 1) * N + j] * a.e0[cls + 1];
+                const real* e0 = a.inst_e0 ? a.inst_e0 + 4 * inst : a.e0;
+                const real eyf = a.ey[cls * N + j] * e0[cls], eyh = a.ey[(cls + 1) * N + j] * e0[cls + 1];
                 // column kx = 0
                 {
                     const size_t idx = (size_t)j * TW;   // tile 0, column 0
@@ -441,8 +455,9 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t,
                 if (k2 > 0) esum += m2 / k2;
             }
         }
-        atomicAdd(&a.diag[0], zsum);
-        atomicAdd(&a.diag[1], esum);
+        double* dg = a.diag + a.diag_istride * inst;
+        atomicAdd(&dg[0], zsum);
+        atomicAdd(&dg[1], esum);
     }
     if (a.mode == MODE_NONL || !a.do_inverse) return;
 
@@ -468,7 +483,7 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int t,
         fft.template run<true>(t, v, x);
         if (active)
 #pragma unroll
-            for (int e = 0; e < E; ++e) a.D[(size_t)p * N + t + TEAM * e] = v[e];
+            for (int e = 0; e < E; ++e) a.D[io + (size_t)p * N + t + TEAM * e] = v[e];
     }
 }
 
@@ -489,16 +504,20 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
     typename K::FFT fft;
     fft.template init<N>(t, a.tw);
     K k{a, fft, t, w, bufs, mbar, 0u, 0, 0, 0, 0, 0, 0, false, false};
+    // item q of the launch: kind-major over instances (all r1+r2 tiles of all
+    // instances first, then the w tiles, then the edge columns)
+    const int total = K::NITEMS * a.ninst;
     for (;;) {
         if (tid == 0) *item_sh = atomicAdd(a.queue, 1);
         __syncthreads();
-        const int item = *item_sh;
+        const int q = *item_sh;
         __syncthreads();
-        if (item >= K::NITEMS) break;
-        if (item < K::TILES) k.item(1, 2, item);
-        else if (item < 2 * K::TILES) k.item(0, -1, item - K::TILES);
+        if (q >= total) break;
+        const int local = q / a.ninst, inst = q % a.ninst;
+        if (local < K::TILES) k.item(1, 2, local, inst);
+        else if (local < 2 * K::TILES) k.item(0, -1, local - K::TILES, inst);
         else {
-            col_edge<real, N, TW, E>(a, item - 2 * K::TILES, t, w, bufs, ctab);
+            col_edge<real, N, TW, E>(a, local - 2 * K::TILES, inst, t, w, bufs, ctab);
             __syncthreads();
         }
     }
@@ -545,9 +564,11 @@ struct RowKernel {
     int n, t;
     X x;
     real* keep;            // [NKEEP][N], point m at [slot][m]
+    int inst;              // instance of this row
+    size_t io;             // its buffer offset (complex elements)
     TeamFFT<real, N, E> fft;
 
-    __device__ cplx<real> yv(int q, int k) const { return a.Y[(size_t)q * N * H + (size_t)n * H + k]; }
+    __device__ cplx<real> yv(int q, int k) const { return a.Y[io + (size_t)q * N * H + (size_t)n * H + k]; }
 
     // half spectrum of physical field p at x wave number k in [1, H)
     __device__ cplx<real> xspec(int p, int k) const {
@@ -575,8 +596,8 @@ struct RowKernel {
 
     // C2R pair: v[e] = (field pa, field pb) at point m = t + TEAM e
     __device__ void c2r(int pa, int pb, cplx<real> (&v)[E]) {
-        const cplx<real> da = a.D[(size_t)pa * N + n];
-        const cplx<real> db = pb >= 0 ? a.D[(size_t)pb * N + n] : mk<real>(0, 0);
+        const cplx<real> da = a.D[io + (size_t)pa * N + n];
+        const cplx<real> db = pb >= 0 ? a.D[io + (size_t)pb * N + n] : mk<real>(0, 0);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int k = t + TEAM * e;
@@ -606,13 +627,13 @@ struct RowKernel {
         }
         if (t == 0) {
             const cplx<real> z0 = x.read(0), zh = x.read(H);
-            if (ep >= 0) a.Ed[(size_t)ep * N + n] = mk<real>(z0.x, zh.x);
-            if (eq >= 0) a.Ed[(size_t)eq * N + n] = mk<real>(z0.y, zh.y);
+            if (ep >= 0) a.Ed[io + (size_t)ep * N + n] = mk<real>(z0.x, zh.x);
+            if (eq >= 0) a.Ed[io + (size_t)eq * N + n] = mk<real>(z0.y, zh.y);
         }
         x.sync();
     }
 
-    __device__ cplx<real>* grow(int g) const { return a.G + (size_t)g * N * H + (size_t)n * H; }
+    __device__ cplx<real>* grow(int g) const { return a.G + io + (size_t)g * N * H + (size_t)n * H; }
     __device__ real& kp(int f, int e) const { return keep[f * N + t + TEAM * e]; }
     __device__ void zero_slot0(int g) const { if (t == 0) grow(g)[0] = mk<real>(0, 0); }
     __device__ void dump(int fld, const cplx<real> (&v)[E], bool imag) const {
@@ -628,7 +649,8 @@ struct RowKernel {
         for (int e = 0; e < E; ++e) o[t + TEAM * e] = kp(slot, e);
     }
     __device__ real alpha_at(int e) const {
-        return a.alpha_field ? a.alpha_field[(size_t)n * N + t + TEAM * e] : a.alpha;
+        if (a.alpha_field) return a.alpha_field[a.alpha_istride * inst + (size_t)n * N + t + TEAM * e];
+        return a.inst_alpha ? a.inst_alpha[inst] : a.alpha;
     }
     __device__ real S_at(int e) const {
         const real r1 = kp(0, e), r2 = kp(1, e);
@@ -764,12 +786,14 @@ struct RowKernel {
 template <typename real, int N, int E, int ROWS, int MINB>
 __global__ void __launch_bounds__(ROWS * (N / E), MINB) row_kernel(const StageArgs<real> a) {
     using K = RowKernel<real, N, E, ROWS>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int r = threadIdx.x / K::TEAM, t = threadIdx.x % K::TEAM;
     unsigned char* mine = smem_raw + (size_t)r * K::SMEM_PER_ROW;
-    K k{a, (int)blockIdx.x * ROWS + r, t,
+    constexpr int BLOCKS_PER_INST = N / ROWS;
+    const int inst = (int)blockIdx.x / BLOCKS_PER_INST;
+    K k{a, ((int)blockIdx.x % BLOCKS_PER_INST) * ROWS + r, t,
         typename K::X{reinterpret_cast<cplx<real>*>(mine), 1 + r},
-        reinterpret_cast<real*>(mine + N * sizeof(cplx<real>)), {}};
+        reinterpret_cast<real*>(mine + N * sizeof(cplx<real>)), inst, (size_t)inst * a.istride, {}};
     static_assert(K::PH * K::TEAM == N / 2, "row team layout");
     k.run();
 }

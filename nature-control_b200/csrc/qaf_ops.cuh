@@ -16,7 +16,7 @@ template <typename real, int N, int W, int E>
 __global__ void __launch_bounds__(W * (N / E))
 col_ifft_kernel(const cplx<real>* __restrict__ spec, cplx<real>* __restrict__ T, const cplx<real>* __restrict__ tw) {
     constexpr int H = N / 2, TEAM = N / E, NXH = H + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<real>* buf = reinterpret_cast<cplx<real>*>(smem_raw);
     const int w = threadIdx.x % W, t = threadIdx.x / W;
     const int i = blockIdx.x * W + w;
@@ -48,7 +48,7 @@ template <typename real, int N, int W, int E>
 __global__ void __launch_bounds__(W * (N / E))
 col_fft_kernel(const cplx<real>* __restrict__ T, cplx<real>* __restrict__ spec, const cplx<real>* __restrict__ tw) {
     constexpr int H = N / 2, TEAM = N / E, NXH = H + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<real>* buf = reinterpret_cast<cplx<real>*>(smem_raw);
     const int w = threadIdx.x % W, t = threadIdx.x / W;
     const int i = blockIdx.x * W + w;
@@ -80,7 +80,7 @@ template <typename real, int N, int E, int ROWS>
 __global__ void __launch_bounds__(ROWS * (N / 2 / E))
 row_c2r_kernel(const cplx<real>* __restrict__ T, real* __restrict__ phys, const cplx<real>* __restrict__ tw) {
     constexpr int H = N / 2, TEAM = H / E;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<real>* buf = reinterpret_cast<cplx<real>*>(smem_raw);
     const int r = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
     const int n = blockIdx.x * ROWS + r;
@@ -114,7 +114,7 @@ template <typename real, int N, int E, int ROWS>
 __global__ void __launch_bounds__(ROWS * (N / 2 / E))
 row_r2c_kernel(const real* __restrict__ phys, cplx<real>* __restrict__ T, const cplx<real>* __restrict__ tw) {
     constexpr int H = N / 2, TEAM = H / E;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<real>* buf = reinterpret_cast<cplx<real>*>(smem_raw);
     const int r = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
     const int n = blockIdx.x * ROWS + r;

@@ -101,6 +101,15 @@ struct alignas(64) StageArgs {
     unsigned* flags;       // StatusFlag bits
     int* queue;            // work counter of the persistent column kernel (reset by the row kernel)
     real* phys_out;        // optional: 9 physical fields + S + p11 p12 p21 (13 * N * N)
+    // batches of independent instances of the same grid: every buffer above
+    // (state, intermediates, D, Ed) of instance k sits istride complex elements
+    // after instance k-1's; per-instance parameters come from the inst_ arrays
+    int ninst;             // instances in the launch (1: a single grid)
+    size_t istride;        // complex elements between instances (a multiple of H)
+    const real* inst_alpha;   // constant activity per instance, or nullptr (alpha)
+    size_t alpha_istride;     // reals between instances' activity fields (0: shared)
+    const real* inst_e0;      // e0[4] per instance, or nullptr (e0)
+    size_t diag_istride;      // doubles between instances' diagnostics (0: shared)
 };
 
 template <typename real>

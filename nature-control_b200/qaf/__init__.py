@@ -36,7 +36,9 @@ EXPORTS = [
     "qaf_xderiv", "qaf_yderiv", "qaf_laplacian", "qaf_vel", "qaf_dealias", "qaf_if_tables", "qaf_integrate",
     "qaf_nonlinear", "qaf_step", "qaf_step_host", "qaf_last_diagnostics", "qaf_check_finite", "qaf_diagnostics",
     "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_state_advance_timed", "qaf_launch_count",
-    "qaf_init_random_q", "qaf_step_noalloc",
+    "qaf_init_random_q", "qaf_step_noalloc", "qaf_ensemble_create", "qaf_ensemble_destroy",
+    "qaf_ensemble_init_random", "qaf_ensemble_load", "qaf_ensemble_store", "qaf_ensemble_advance",
+    "qaf_ensemble_diagnostics", "qaf_ensemble_set_controls",
 ]
 
 
@@ -124,6 +126,17 @@ def lib():
         L.qaf_init_random_q.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp]
         L.qaf_step_noalloc.argtypes = [cp, ctypes.c_double, ctypes.c_double, cp, ctypes.POINTER(CParams), cp,
                                        vp, vp, vp, cp, vp]
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.qaf_ensemble_create.argtypes = [cp, ctypes.POINTER(cp), ctypes.c_double, ctypes.c_double, cp,
+                                          ctypes.POINTER(CParams), dp, dp, ctypes.POINTER(vp)]
+        L.qaf_ensemble_destroy.argtypes = [vp]
+        L.qaf_ensemble_init_random.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_double,
+                                               ctypes.c_double, vp]
+        L.qaf_ensemble_load.argtypes = [vp, cp, vp, vp, vp, vp]
+        L.qaf_ensemble_store.argtypes = [vp, cp, vp, vp, vp, vp]
+        L.qaf_ensemble_advance.argtypes = [vp, cp, vp]
+        L.qaf_ensemble_diagnostics.argtypes = [vp, dp, vp]
+        L.qaf_ensemble_set_controls.argtypes = [vp, dp, dp, vp]
         _lib = L
     return _lib
 
@@ -343,3 +356,84 @@ class Mesh:
         _check(lib().qaf_diagnostics(self._h, self._chk_spec(w), ctypes.byref(e), ctypes.byref(z),
                                      spec.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nshells, _stream()))
         return e.value, z.value, (spec[:nshells] if nshells else None)
+
+
+class Ensemble:
+    """Many independent instances advanced together with IF-RK4.
+
+    Instance k has grid n[k] x n[k] (one of the supported sizes), activity
+    alpha[k] and friction rf[k]; Re, Er, lambda, dt and q_lin come from the
+    shared Params. The reference runs one grid per process (friction.cu);
+    this is the batched form of that loop.
+    """
+
+    def __init__(self, n, p: Params, alpha, rf=None, lx: float = 2 * math.pi, ly: Optional[float] = None,
+                 dtype: int = F32):
+        self.n = [int(v) for v in n]
+        k = len(self.n)
+        self.alpha = [float(v) for v in alpha]
+        self.rf = [float(p.rf)] * k if rf is None else [float(v) for v in rf]
+        if len(self.alpha) != k or len(self.rf) != k:
+            raise ValueError("alpha and rf need one value per instance")
+        self.lx, self.ly, self.dtype, self.params = lx, ly or lx, dtype, p
+        self._meshes = {}
+        cp = p.c()
+        h = ctypes.c_void_p()
+        na = (ctypes.c_int * k)(*self.n)
+        aa = (ctypes.c_double * k)(*self.alpha)
+        ra = (ctypes.c_double * k)(*self.rf)
+        _check(lib().qaf_ensemble_create(k, na, self.lx, self.ly, dtype, ctypes.byref(cp), aa, ra, ctypes.byref(h)))
+        self._h = h
+
+    def __len__(self):
+        return len(self.n)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.qaf_ensemble_destroy(h)
+            self._h = None
+
+    def mesh(self, k: int) -> Mesh:
+        """A Mesh with instance k's geometry (for tensors and transforms)."""
+        n = self.n[k]
+        if n not in self._meshes:
+            self._meshes[n] = Mesh(n, n, self.lx, self.ly, self.dtype)
+        return self._meshes[n]
+
+    def init_random(self, seeds, lo: float = -0.01, hi: float = 0.01):
+        sa = (ctypes.c_uint64 * len(self.n))(*[int(v) for v in seeds])
+        _check(lib().qaf_ensemble_init_random(self._h, sa, lo, hi, _stream()))
+
+    def load(self, k: int, w, r1, r2):
+        m = self.mesh(k)
+        _check(lib().qaf_ensemble_load(self._h, k, m._chk_spec(w), m._chk_spec(r1), m._chk_spec(r2), _stream()))
+
+    def store(self, k: int):
+        m = self.mesh(k)
+        w, r1, r2 = m.new_spec(), m.new_spec(), m.new_spec()
+        _check(lib().qaf_ensemble_store(self._h, k, m._chk_spec(w), m._chk_spec(r1), m._chk_spec(r2), _stream()))
+        return w, r1, r2
+
+    def advance(self, nsteps: int = 1):
+        _check(lib().qaf_ensemble_advance(self._h, nsteps, _stream()))
+
+    def set_controls(self, alpha, rf=None):
+        """New per-instance activity (and friction) for the following steps."""
+        k = len(self.n)
+        alpha = [float(v) for v in alpha]
+        rf = self.rf if rf is None else [float(v) for v in rf]
+        if len(alpha) != k or len(rf) != k:
+            raise ValueError("alpha and rf need one value per instance")
+        self.alpha, self.rf = alpha, rf
+        aa = (ctypes.c_double * k)(*self.alpha)
+        ra = (ctypes.c_double * k)(*self.rf)
+        _check(lib().qaf_ensemble_set_controls(self._h, aa, ra, _stream()))
+
+    def diagnostics(self):
+        """[(energy, enstrophy)] per instance after the last step."""
+        k = len(self.n)
+        out = (ctypes.c_double * (2 * k))()
+        _check(lib().qaf_ensemble_diagnostics(self._h, out, _stream()))
+        return [(out[2 * i], out[2 * i + 1]) for i in range(k)]
+
