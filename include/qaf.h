@@ -198,6 +198,31 @@ qaf_status qaf_ensemble_set_controls(qaf_ensemble* ens, const double* alpha, con
 /* synchronises `stream`; out[2k], out[2k+1] = energy, enstrophy of instance k after the last step */
 qaf_status qaf_ensemble_diagnostics(qaf_ensemble* ens, double* out, void* stream);
 
+/* ---- discrete adjoint (IF-RK4) ---------------------------------------------
+ * No counterpart in the reference (it has no gradients): reverse-mode
+ * derivatives of `nsteps` IF-RK4 steps (qaf_state_advance) with respect to the
+ * initial spectra and the activity field Ra(x). The loss is
+ *     L = (1/loss_window) * sum of the enstrophy (as qaf_last_diagnostics) of
+ *         the states after the last loss_window steps      (0: no loss term)
+ * and/or any function of the final state through its gradient.
+ * qaf_adjoint_create: allocates checkpoints every `checkpoint_every` steps and
+ *   the recording of one segment (4 * checkpoint_every * 9 physical fields);
+ *   borrows `mesh`, whose resident state the calls below overwrite.
+ * qaf_adjoint_forward: runs the steps from (w0, r1_0, r2_0) (reference-layout
+ *   device spectra) with params p (p->alpha_field must stay valid until the
+ *   backward call); optional final state out; *loss on return (synchronises).
+ * qaf_adjoint_backward: gwT/gr1T/gr2T = dL/d(final state) or NULL (zero),
+ *   gloss = dL/d(loss); writes dL/d(initial spectra) (NULL: skipped) and
+ *   dL/dRa(x) (nx*ny reals, NULL: skipped). Gradients of complex entries are
+ *   dL/dRe + i dL/dIm. */
+typedef struct qaf_adjoint qaf_adjoint;
+qaf_status qaf_adjoint_create(qaf_mesh* mesh, int nsteps, int checkpoint_every, int loss_window, qaf_adjoint** out);
+qaf_status qaf_adjoint_destroy(qaf_adjoint* adj);
+qaf_status qaf_adjoint_forward(qaf_adjoint* adj, const qaf_params* p, const void* w0, const void* r1_0,
+                               const void* r2_0, void* wT, void* r1T, void* r2T, double* loss, void* stream);
+qaf_status qaf_adjoint_backward(qaf_adjoint* adj, const void* gwT, const void* gr1T, const void* gr2T, double gloss,
+                                void* gw0, void* gr1_0, void* gr2_0, void* galpha, void* stream);
+
 /* ---- allocation-free step --------------------------------------------------
  * No counterpart in the reference (whose Mesh and Field always cudaMalloc).
  * For callers that cannot allocate device memory when they step — work

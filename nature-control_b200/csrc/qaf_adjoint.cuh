@@ -1,0 +1,460 @@
+// qaf_adjoint.cuh — discrete adjoint of the IF-RK4 step (two kernels per stage).
+//
+// The forward map of one step is the reference's literal sequence
+// (friction.cu:212-259 with RK4.cuh:12-74 and the nonlinear terms of
+// friction/Qsolver.cuh:63-312): spectral multipliers, BwdTrans B = C2R / N^2
+// (with the Hermitian projection P of the kx = 0 and kx = N/2 columns that
+// cufftExecZ2D applies), pointwise products, FwdTrans F = R2C. Every piece but
+// the products is real-linear; under the real inner product
+// <a, b> = Re sum conj(a) b over the stored half spectrum
+//     F^T(a) = C2R(W a)            W = 1 on the edge columns, 1/2 elsewhere
+//     B^T(y) = c R2C(y) / N^2      c = 1 on the edge columns, 2 elsewhere
+//     (m .)^T = conj(m) .,  P^T = P,
+// so the adjoint of a stage's nonlinear term is (spectral) 11 multiplied
+// y-iFFTs -> (row) 11 C2R, the transposed products against the forward
+// fields of that stage, 9 R2C -> (spectral) 9 y-FFTs combined with the
+// conjugate multipliers. The column kernel also carries the RK4 adjoint
+// recursion, so one column launch ends stage s and starts stage s - 1.
+//
+// With a = M sbar(n+1) (M the 2/3 mask) and E, Eh the full and half-step
+// integrating factors of each field, the IF-RK4 adjoint is
+//     kb4 = dt/6 a                         cb4 = VJP(c4, kb4)
+//     kb3 = dt Eh cb4 + dt/3 Eh a          cb3 = VJP(c3, kb3)
+//     kb2 = dt/2 cb3 + dt/3 Eh a           cb2 = VJP(c2, kb2)
+//     kb1 = dt/2 Eh cb2 + dt/6 E a         cb1 = VJP(c1, kb1)
+//     sbar(n) = E a + E cb4 + Eh cb3 + Eh cb2 + cb1   (+ the loss term of s(n)).
+#pragma once
+
+#include "qaf_stage.cuh"
+
+namespace qaf {
+
+// adjoint physical inputs g_q = C2R(W m_q lambda) of the products, in the
+// order the forward's nonlinear terms are formed
+enum AdjIn : int {
+    GA_UW = 0,   // -u w   (wnonl advection, x part; projected)
+    GA_VW,       // -v w   (y part; projected)
+    GA_P11,      // p11 -> 2 ce kx ky
+    GA_P12,      // p12 -> -ce kx^2
+    GA_P21,      // p21 -> ce ky^2
+    GA_A1,       // -w r2 - S^2 r1 + lambda S du/dx   (r1nonl)
+    GA_UR1,      // -u r1  -> i kx
+    GA_VR1,      // -v r1  -> i ky
+    GA_A2,       // w r1 - S^2 r2 + lambda/2 S (du/dy + dv/dx)   (r2nonl)
+    GA_UR2,      // -u r2
+    GA_VR2,      // -v r2
+    NGA
+};
+
+template <typename real>
+struct AdjArgs {
+    real dkx, dky, dt, lambda, ce;
+    int advect, kx_keep, ky_lo, ky_hi;
+    const cplx<real>* tw;
+    const real* ex;
+    const real* ey;
+    real e0[4];
+    cplx<real>* Tg;            // NGA arrays of N*H: column kernel -> row kernel
+    cplx<real>* Tx;            // PF_COUNT arrays of N*H: row kernel -> column kernel
+    cplx<real>* abar[3];       // M sbar(n+1), reference layout
+    cplx<real>* sacc[3];       // partial sums of sbar(n)
+    cplx<real>* sbar[3];       // the adjoint state
+    cplx<real>* edge;          // 6 * N scratch: kb of the kx = 0 and kx = N/2 columns
+    const cplx<real>* wstate;  // w of the state whose adjoint completes in this launch (loss term) or nullptr
+    real loss_w;               // d loss / d enstrophy of that state
+    int stage;                 // 4..1: Tx holds the transposed products of this stage; 0: start from sbar
+    int emit;                  // write Tg for the stage before
+    const real* phys;          // the stage input's forward fields (PhysField order, N*N each)
+    const real* alpha_field;   // activity field or nullptr (alpha)
+    real alpha;
+    real* alpha_grad;          // += d loss / d alpha(x), or nullptr
+};
+
+// conj(multiplier) of the forward field p (derived()) applied to the transform of its adjoint
+template <typename real>
+__device__ __forceinline__ void adj_combine(int p, cplx<real> v, real kx, real ky, real ik2, cplx<real>& cw,
+                                            cplx<real>& c1, cplx<real>& c2) {
+    switch (p) {
+        case PF_W: cw = cadd(cw, v); break;
+        case PF_R1: c1 = cadd(c1, v); break;
+        case PF_R2: c2 = cadd(c2, v); break;
+        case PF_U: cw = cadd(cw, cmul_mi(cscale(v, ky * ik2))); break;        // conj(i ky / k^2)
+        case PF_V: cw = cadd(cw, cmul_i(cscale(v, kx * ik2))); break;         // conj(-i kx / k^2)
+        case PF_UX: cw = cadd(cw, cscale(v, -kx * ky * ik2)); break;
+        case PF_SH: cw = cadd(cw, cscale(v, (kx * kx - ky * ky) * ik2)); break;
+        case PF_LR1: c1 = cadd(c1, cscale(v, -(kx * kx + ky * ky))); break;
+        default: c2 = cadd(c2, cscale(v, -(kx * kx + ky * ky))); break;   // PF_LR2
+    }
+}
+
+// conj(multiplier) that maps the nonlinear adjoint lambda of field f(q) to g_q's spectrum
+template <typename real>
+__device__ __forceinline__ cplx<real> adj_emit(int q, cplx<real> lw, cplx<real> l1, cplx<real> l2, real kx, real ky,
+                                               real ce) {
+    switch (q) {
+        case GA_UW: return cmul_mi(cscale(lw, kx));
+        case GA_VW: return cmul_mi(cscale(lw, ky));
+        case GA_P11: return cscale(lw, 2 * ce * kx * ky);
+        case GA_P12: return cscale(lw, -ce * kx * kx);
+        case GA_P21: return cscale(lw, ce * ky * ky);
+        case GA_A1: return l1;
+        case GA_UR1: return cmul_mi(cscale(l1, kx));
+        case GA_VR1: return cmul_mi(cscale(l1, ky));
+        case GA_A2: return l2;
+        case GA_UR2: return cmul_mi(cscale(l2, kx));
+        default: return cmul_mi(cscale(l2, ky));                          // GA_VR2
+    }
+}
+
+// The RK4 adjoint recursion at one spectral point of field f. cb: the VJP of
+// the stage (unused at stage 0); returns the nonlinear adjoint kb of the
+// stage before. lossg: the loss gradient of the state completed here.
+template <typename real>
+__device__ __forceinline__ cplx<real> adj_rk(const AdjArgs<real>& a, int f, size_t idx, cplx<real> cb, real E,
+                                             real Eh, bool keep, cplx<real> lossg) {
+    const real dt = a.dt;
+    const real sixth = (real)(1.0 / 6.0), third = (real)(1.0 / 3.0), half = (real)0.5;
+    cplx<real> sb;
+    if (a.stage == 0) {
+        sb = cadd(pick3(a.sbar, f)[idx], lossg);
+    } else if (a.stage == 1) {
+        sb = cadd(cadd(pick3(a.sacc, f)[idx], cb), lossg);
+        pick3(a.sbar, f)[idx] = sb;
+    } else {
+        const cplx<real> av = pick3(a.abar, f)[idx];
+        cplx<real> sc = pick3(a.sacc, f)[idx];
+        cplx<real> kb;
+        if (a.stage == 4) {
+            sc = cadd(sc, cscale(cb, E));
+            kb = cadd(cscale(cb, dt * Eh), cscale(av, third * dt * Eh));
+        } else if (a.stage == 3) {
+            sc = cadd(sc, cscale(cb, Eh));
+            kb = cadd(cscale(cb, half * dt), cscale(av, third * dt * Eh));
+        } else {
+            sc = cadd(sc, cscale(cb, Eh));
+            kb = cadd(cscale(cb, half * dt * Eh), cscale(av, sixth * dt * E));
+        }
+        pick3(a.sacc, f)[idx] = sc;
+        return kb;
+    }
+    // stages 0 and 1 start the step before: a = M sbar, sacc = E a, kb4 = dt/6 a
+    if (!a.emit) return mk<real>(0, 0);
+    const cplx<real> av = keep ? sb : mk<real>(0, 0);
+    pick3(a.abar, f)[idx] = av;
+    pick3(a.sacc, f)[idx] = cscale(av, E);
+    return cscale(av, sixth * dt);
+}
+
+template <typename real, int N>
+__device__ __forceinline__ void adj_factors(const AdjArgs<real>& a, int f, int i, int j, real& E, real& Eh) {
+    constexpr int H = N / 2;
+    const int cls = f == 0 ? 0 : 2;
+    E = a.ex[cls * (H + 1) + i] * a.e0[cls] * a.ey[cls * N + j];
+    Eh = a.ex[(cls + 1) * (H + 1) + i] * a.e0[cls + 1] * a.ey[(cls + 1) * N + j];
+}
+
+template <typename real>
+__device__ __forceinline__ bool adj_keep(const AdjArgs<real>& a, int i, int j) {
+    return i <= a.kx_keep && (j <= a.ky_lo || j >= a.ky_hi);
+}
+
+// kx = 0 and kx = N/2 columns (packed in slot 0 of the T arrays as DC + i Nyquist), by the first team of the last block
+template <typename real, int N, int W, int E>
+__device__ void adj_col_edge(const AdjArgs<real>& a, const TeamFFT<real, N, E>& fft, cplx<real>* buf, int w, int t) {
+    constexpr int H = N / 2, TEAM = N / E, NXH = H + 1;
+    XchgCols<real> x{buf, w, W};
+    const bool lead = w == 0;
+    const real kN = a.dkx * (real)H;
+    const real sc = (real)1 / ((real)N * (real)N);
+    const real n4 = sc * sc;
+#pragma unroll 1
+    for (int c = 0; c < 2; ++c) {
+        const int i = c == 0 ? 0 : H;
+        const real kx = c == 0 ? (real)0 : kN;
+        cplx<real> cw[E], c1[E], c2[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) { cw[e] = mk<real>(0, 0); c1[e] = cw[e]; c2[e] = cw[e]; }
+        if (a.stage >= 1) {
+#pragma unroll 1
+            for (int p = 0; p < PF_COUNT; ++p) {
+                cplx<real> v[E];
+#pragma unroll
+                for (int e = 0; e < E; ++e)
+                    v[e] = lead ? a.Tx[(size_t)p * N * H + (size_t)(t + TEAM * e) * H] : mk<real>(0, 0);
+                fft.template run<false>(t, v, x);
+#pragma unroll
+                for (int e = 0; e < E; ++e) x.write(t + TEAM * e, v[e]);
+                x.sync();
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int j = t + TEAM * e;
+                    const cplx<real> zm = cconj(x.read((N - j) % N));
+                    const cplx<real> z = c == 0 ? cscale(cadd(v[e], zm), (real)0.5)
+                                                : cmul_mi(cscale(csub(v[e], zm), (real)0.5));
+                    const real ky = ky_of<real>(j, N, a.dky);
+                    const real k2 = kx * kx + ky * ky;
+                    adj_combine<real>(p, z, kx, ky, k2 > 0 ? (real)1 / k2 : (real)0, cw[e], c1[e], c2[e]);
+                }
+                x.sync();
+            }
+        }
+        if (lead) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int j = t + TEAM * e, jm = (N - j) % N;
+                const size_t idx = (size_t)j * NXH + i;
+                cplx<real> lossg = mk<real>(0, 0);
+                if (a.wstate) {
+                    const cplx<real> P = cscale(cadd(a.wstate[idx], cconj(a.wstate[(size_t)jm * NXH + i])), (real)0.5);
+                    lossg = cscale(P, a.loss_w * n4);
+                }
+                const bool keep = adj_keep(a, i, j);
+                cplx<real> cb[3] = {cscale(cw[e], sc), cscale(c1[e], sc), cscale(c2[e], sc)};
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                    real Ef, Eh;
+                    adj_factors<real, N>(a, f, i, j, Ef, Eh);
+                    const cplx<real> kb = adj_rk(a, f, idx, cb[f], Ef, Eh, keep, f == 0 ? lossg : mk<real>(0, 0));
+                    a.edge[(size_t)(f * 2 + c) * N + j] = kb;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (!a.emit) return;
+#pragma unroll 1
+    for (int q = 0; q < NGA; ++q) {
+        if (!a.advect && q <= GA_VW) continue;
+        cplx<real> v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            v[e] = mk<real>(0, 0);
+            if (!lead) continue;
+            const int j = t + TEAM * e;
+            cplx<real> P[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const real kx = c == 0 ? (real)0 : kN;
+                cplx<real> val[2];
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int jj = s == 0 ? j : (N - j) % N, jp = (N - jj) % N;
+                    cplx<real> lw = a.edge[(size_t)c * N + jj];
+                    if (q <= GA_VW)   // the advection terms are projected before the derivative's adjoint
+                        lw = cscale(cadd(lw, cconj(a.edge[(size_t)c * N + jp])), (real)0.5);
+                    const cplx<real> l1 = a.edge[(size_t)(2 + c) * N + jj], l2 = a.edge[(size_t)(4 + c) * N + jj];
+                    val[s] = adj_emit<real>(q, lw, l1, l2, kx, ky_of<real>(jj, N, a.dky), a.ce);
+                }
+                P[c] = cscale(cadd(val[0], cconj(val[1])), (real)0.5);
+            }
+            v[e] = cadd(P[0], cmul_i(P[1]));
+        }
+        fft.template run<true>(t, v, x);
+        if (lead)
+#pragma unroll
+            for (int e = 0; e < E; ++e) a.Tg[(size_t)q * N * H + (size_t)(t + TEAM * e) * H] = v[e];
+    }
+}
+
+// One team of N/E threads per kx-column i in [1, H); the last block takes the edge columns.
+template <typename real, int N, int W, int E>
+__global__ void __launch_bounds__(W * (N / E)) adj_col_kernel(const __grid_constant__ AdjArgs<real> a) {
+    constexpr int H = N / 2, TEAM = N / E, NXH = H + 1;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cplx<real>* buf = reinterpret_cast<cplx<real>*>(smem_raw);
+    const int w = threadIdx.x % W, t = threadIdx.x / W;
+    TeamFFT<real, N, E> fft;
+    fft.template init<N>(t, a.tw);
+    if (blockIdx.x == gridDim.x - 1) {
+        adj_col_edge<real, N, W, E>(a, fft, buf, w, t);
+        return;
+    }
+    const int i = blockIdx.x * W + w;
+    const bool active = i != 0;
+    XchgCols<real> x{buf, w, W};
+    const real kx = a.dkx * (real)i;
+    const real sc = (real)2 / ((real)N * (real)N);
+    cplx<real> cw[E], c1[E], c2[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) { cw[e] = mk<real>(0, 0); c1[e] = cw[e]; c2[e] = cw[e]; }
+    if (a.stage >= 1) {
+#pragma unroll 1
+        for (int p = 0; p < PF_COUNT; ++p) {
+            cplx<real> v[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+                v[e] = active ? a.Tx[(size_t)p * N * H + (size_t)(t + TEAM * e) * H + i] : mk<real>(0, 0);
+            fft.template run<false>(t, v, x);
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const real ky = ky_of<real>(t + TEAM * e, N, a.dky);
+                const real k2 = kx * kx + ky * ky;
+                adj_combine<real>(p, v[e], kx, ky, k2 > 0 ? (real)1 / k2 : (real)0, cw[e], c1[e], c2[e]);
+            }
+        }
+    }
+    if (active) {
+        const real n4 = (real)1 / ((real)N * (real)N) / ((real)N * (real)N);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int j = t + TEAM * e;
+            const size_t idx = (size_t)j * NXH + i;
+            const bool keep = adj_keep(a, i, j);
+            const cplx<real> lossg = a.wstate ? cscale(a.wstate[idx], 2 * a.loss_w * n4) : mk<real>(0, 0);
+            real Ef, Eh;
+            adj_factors<real, N>(a, 0, i, j, Ef, Eh);
+            cw[e] = adj_rk(a, 0, idx, cscale(cw[e], sc), Ef, Eh, keep, lossg);
+            adj_factors<real, N>(a, 1, i, j, Ef, Eh);
+            c1[e] = adj_rk(a, 1, idx, cscale(c1[e], sc), Ef, Eh, keep, mk<real>(0, 0));
+            c2[e] = adj_rk(a, 2, idx, cscale(c2[e], sc), Ef, Eh, keep, mk<real>(0, 0));
+        }
+    }
+    if (!a.emit) return;
+#pragma unroll 1
+    for (int q = 0; q < NGA; ++q) {
+        if (!a.advect && q <= GA_VW) continue;
+        cplx<real> v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const real ky = ky_of<real>(t + TEAM * e, N, a.dky);
+            v[e] = active ? cscale(adj_emit<real>(q, cw[e], c1[e], c2[e], kx, ky, a.ce), (real)0.5) : mk<real>(0, 0);
+        }
+        fft.template run<true>(t, v, x);
+        if (active)
+#pragma unroll
+            for (int e = 0; e < E; ++e) a.Tg[(size_t)q * N * H + (size_t)(t + TEAM * e) * H + i] = v[e];
+    }
+}
+
+// One team of H/E threads per physical row n (half-length real transforms):
+// 11 C2R of the g rows, the transposed products at each point, 9 R2C.
+template <typename real, int N, int E, int ROWS>
+__global__ void __launch_bounds__(ROWS * (N / 2 / E)) adj_row_kernel(const __grid_constant__ AdjArgs<real> a) {
+    constexpr int H = N / 2, TEAM = H / E;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cplx<real>* xb = reinterpret_cast<cplx<real>*>(smem_raw);
+    const int r = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
+    const int n = blockIdx.x * ROWS + r;
+    XchgRow<real> x{xb + r * H};
+    real* gs = reinterpret_cast<real*>(xb + ROWS * H) + (size_t)r * NGA * N;
+    TeamFFT<real, H, E> fft;
+    fft.template init<N>(t, a.tw);
+
+    // 1. g_q rows by C2R (slot 0 of each T row holds DC + i Nyquist)
+#pragma unroll 1
+    for (int q = 0; q < NGA; ++q) {
+        if (!a.advect && q <= GA_VW) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int m = t + TEAM * e;
+                gs[q * N + 2 * m] = 0;
+                gs[q * N + 2 * m + 1] = 0;
+            }
+            continue;
+        }
+        const cplx<real>* row = a.Tg + (size_t)q * N * H + (size_t)n * H;
+        cplx<real> v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int k = t + TEAM * e;
+            if (k == 0) {
+                const cplx<real> d = row[0];
+                v[e] = mk<real>(d.x + d.y, d.x - d.y);
+            } else {
+                const cplx<real> A = row[k], B = cconj(row[H - k]);
+                v[e] = cadd(cadd(A, B), cmul_i(cmul(cconj(a.tw[k]), csub(A, B))));
+            }
+        }
+        fft.template run<true>(t, v, x);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int m = t + TEAM * e;
+            gs[q * N + 2 * m] = v[e].x;
+            gs[q * N + 2 * m + 1] = v[e].y;
+        }
+    }
+
+    // 2. transposed products; the adjoints overwrite slots 0..8 of this point
+    const real lam = a.lambda;
+    const size_t rb = (size_t)n * N;
+    const size_t NN = (size_t)N * N;
+#pragma unroll 1
+    for (int e = 0; e < E; ++e) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int xi = 2 * (t + TEAM * e) + h;
+            const size_t pi = rb + xi;
+            const real w = a.phys[PF_W * NN + pi], r1 = a.phys[PF_R1 * NN + pi], r2 = a.phys[PF_R2 * NN + pi];
+            const real u = a.phys[PF_U * NN + pi], v = a.phys[PF_V * NN + pi], ux = a.phys[PF_UX * NN + pi];
+            const real sh = a.phys[PF_SH * NN + pi], L1 = a.phys[PF_LR1 * NN + pi], L2 = a.phys[PF_LR2 * NN + pi];
+            const real al = a.alpha_field ? a.alpha_field[pi] : a.alpha;
+            real g[NGA];
+#pragma unroll
+            for (int q = 0; q < NGA; ++q) g[q] = gs[q * N + xi];
+            const real S = 2 * sqrt(r1 * r1 + r2 * r2);
+            const real sgl = lam * S * (S * S - 1);
+            const real dsgl = lam * (3 * S * S - 1);
+            const real g1221 = g[GA_P12] + g[GA_P21];
+            const real Sb = (-lam * L1 + dsgl * r1) * g[GA_P11] + (-lam * L2 + dsgl * r2) * g1221 +
+                            (-2 * S * r1 + lam * ux) * g[GA_A1] + (-2 * S * r2 + (real)0.5 * lam * sh) * g[GA_A2];
+            const real dS1 = S > 0 ? 4 * r1 / S : (real)0, dS2 = S > 0 ? 4 * r2 / S : (real)0;
+            const real wb = -u * g[GA_UW] - v * g[GA_VW] - r2 * g[GA_A1] + r1 * g[GA_A2];
+            const real r1b = (sgl - al) * g[GA_P11] - 2 * L2 * g[GA_P12] + 2 * L2 * g[GA_P21] - S * S * g[GA_A1] -
+                             u * g[GA_UR1] - v * g[GA_VR1] + w * g[GA_A2] + Sb * dS1;
+            const real r2b = (sgl + 2 * L1 - al) * g[GA_P12] + (sgl - 2 * L1 - al) * g[GA_P21] - w * g[GA_A1] -
+                             S * S * g[GA_A2] - u * g[GA_UR2] - v * g[GA_VR2] + Sb * dS2;
+            const real ub = -w * g[GA_UW] - r1 * g[GA_UR1] - r2 * g[GA_UR2];
+            const real vb = -w * g[GA_VW] - r1 * g[GA_VR1] - r2 * g[GA_VR2];
+            const real uxb = lam * S * g[GA_A1];
+            const real shb = (real)0.5 * lam * S * g[GA_A2];
+            const real L1b = -lam * S * g[GA_P11] + 2 * r2 * g[GA_P12] - 2 * r2 * g[GA_P21];
+            const real L2b = (-lam * S - 2 * r1) * g[GA_P12] + (-lam * S + 2 * r1) * g[GA_P21];
+            if (a.alpha_grad) a.alpha_grad[pi] += -(r1 * g[GA_P11] + r2 * g1221);
+            gs[PF_W * N + xi] = wb;
+            gs[PF_R1 * N + xi] = r1b;
+            gs[PF_R2 * N + xi] = r2b;
+            gs[PF_U * N + xi] = ub;
+            gs[PF_V * N + xi] = vb;
+            gs[PF_UX * N + xi] = uxb;
+            gs[PF_SH * N + xi] = shb;
+            gs[PF_LR1 * N + xi] = L1b;
+            gs[PF_LR2 * N + xi] = L2b;
+        }
+    }
+
+    // 3. R2C of the 9 adjoints into Tx (slot 0: DC + i Nyquist)
+#pragma unroll 1
+    for (int p = 0; p < PF_COUNT; ++p) {
+        cplx<real> v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int m = t + TEAM * e;
+            v[e] = mk<real>(gs[p * N + 2 * m], gs[p * N + 2 * m + 1]);
+        }
+        fft.template run<false>(t, v, x);
+#pragma unroll
+        for (int e = 0; e < E; ++e) x.write(t + TEAM * e, v[e]);
+        x.sync();
+        cplx<real>* out = a.Tx + (size_t)p * N * H + (size_t)n * H;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int k = t + TEAM * e;
+            const cplx<real> zm = cconj(x.read((H - k) % H));
+            if (k == 0) {
+                out[0] = mk<real>(v[e].x + v[e].y, v[e].x - v[e].y);
+            } else {
+                const cplx<real> sum = cscale(cadd(v[e], zm), (real)0.5);
+                const cplx<real> dif = cscale(csub(v[e], zm), (real)0.5);
+                out[k] = csub(sum, cmul_i(cmul(a.tw[k], dif)));
+            }
+        }
+        x.sync();
+    }
+}
+
+// loss += weight * (0.5 / N^4) * diag[0] (the enstrophy sum of the step's new state); weight carries 1/N^4
+__global__ void adj_loss_accumulate(const double* diag, double* loss, double weight) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *loss += weight * 0.5 * diag[0];
+}
+
+}  // namespace qaf

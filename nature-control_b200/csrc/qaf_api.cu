@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>   // PFN_cuTensorMapEncodeTiled
 #include "qaf_kernels.cuh"
 #include "qaf_ops.cuh"
+#include "qaf_adjoint.cuh"
 
 #include <cmath>
 #include <cstdio>
@@ -417,6 +418,7 @@ struct OpNonlinear {
         m->launches += 9;
         StageArgs<real> a = make_args<real>(m, p);
         a.phys_out = static_cast<real*>(phys_out);
+        a.phys_all = 1;
         a.mode = MODE_PROLOGUE; a.do_inverse = 1;
         QAF_CUDA(cudaMemsetAsync(w.queue, 0, sizeof(int), st));
         Launch<real, N>::col(a, st);
@@ -1527,3 +1529,286 @@ qaf_status qaf_ensemble_init_random(qaf_ensemble* e, const uint64_t* seeds, doub
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Discrete adjoint of IF-RK4 (gradients of a mean-enstrophy loss and of the
+// final state with respect to the initial spectra and the activity field).
+// The forward run keeps the state every K steps; the backward sweep, segment
+// by segment from the last, reruns the segment's K steps from its checkpoint
+// recording each stage input's nine physical fields and the vorticity after
+// each step, then walks the steps backwards through the adjoint kernels.
+// ===========================================================================
+struct qaf_adjoint {
+    qaf_mesh* m = nullptr;
+    int nsteps = 0, K = 0, window = 0, nseg = 0;
+    size_t ns = 0, np = 0, rb = 0;
+    unsigned char* blk = nullptr;
+    unsigned char *ckpt = nullptr, *wlog = nullptr, *phys = nullptr, *Tg = nullptr, *Tx = nullptr;
+    unsigned char *abar = nullptr, *sacc = nullptr, *sbar = nullptr, *edge = nullptr, *agrad = nullptr;
+    double* loss = nullptr;
+    qaf_params p{};
+    bool have_forward = false;
+};
+
+namespace {
+
+// what a recording advance keeps
+struct AdjRecord {
+    void* phys;           // 4 slots of PF_COUNT * N * N reals per step, or nullptr
+    void* wlog;           // w after each step (reference layout), or nullptr
+    double* loss;         // += weight * enstrophy sum of the state after each step >= loss_from
+    int loss_from;
+    double loss_weight;
+};
+
+// IF-RK4 steps of the resident state, as OpAdvance, with the recording above
+struct OpRecord {
+    template <typename real, int N>
+    static qaf_status run(qaf_mesh* m, const qaf_params* p, int nsteps, const AdjRecord* rec, cudaStream_t st) {
+        QAF_TRY(ensure_ws<real>(m));
+        QAF_TRY((Launch<real, N>::setup()));
+        QAF_TRY(ensure_if<real>(m, p, st));
+        Workspace<real>& w = ws<real>(m);
+        StageArgs<real> a = make_args<real>(m, p);
+        a.integrator = INT_IFRK4;
+        if (!m->y_valid) {
+            a.mode = MODE_PROLOGUE; a.do_inverse = 1;
+            QAF_CUDA(cudaMemsetAsync(w.queue, 0, sizeof(int), st));
+            Launch<real, N>::col(a, st);
+            m->launches += 1;
+        }
+        a.mode = MODE_STAGE;
+        a.do_inverse = 1;
+        const size_t slot = (size_t)PF_COUNT * N * N;
+        const size_t ns = (size_t)(N / 2 + 1) * N;
+        for (int s = 0; s < nsteps; ++s) {
+            const bool lstep = rec->loss && s >= rec->loss_from;
+            if (lstep) QAF_CUDA(cudaMemsetAsync(w.diag, 0, 2 * sizeof(double), st));
+            for (int k = 1; k <= 4; ++k) {
+                a.stage = k;
+                a.last_stage = k == 4;
+                a.diag = (lstep && k == 4) ? w.diag : nullptr;
+                a.phys_out = rec->phys ? static_cast<real*>(rec->phys) + ((size_t)s * 4 + (k - 1)) * slot : nullptr;
+                Launch<real, N>::row(a, st);
+                Launch<real, N>::col(a, st);
+                m->launches += 2;
+            }
+            if (lstep) { adj_loss_accumulate<<<1, 32, 0, st>>>(w.diag, rec->loss, rec->loss_weight); m->launches += 1; }
+            if (rec->wlog) {
+                from_internal<real>(m, w.old_m[0], w.old_n[0], static_cast<cplx<real>*>(rec->wlog) + (size_t)s * ns, st);
+                m->launches += 1;
+            }
+        }
+        m->y_valid = true;
+        return post_launch("adjoint recording advance");
+    }
+};
+
+template <typename real>
+cplx<real>* adj_field(unsigned char* base, size_t ns, int f) { return reinterpret_cast<cplx<real>*>(base) + (size_t)f * ns; }
+
+struct OpAdjForward {
+    template <typename real, int N>
+    static qaf_status run(qaf_adjoint* A, const void* const* s0, void* const* sT, double* loss, cudaStream_t st) {
+        qaf_mesh* m = A->m;
+        const size_t ns = A->ns, cb = sizeof(cplx<real>);
+        for (int f = 0; f < 3; ++f)
+            QAF_CUDA(cudaMemcpyAsync(adj_field<real>(A->ckpt, ns, f), s0[f], ns * cb, cudaMemcpyDeviceToDevice, st));
+        QAF_TRY((OpLoad::run<real, N>(m, const_cast<void* const*>(s0), st)));
+        QAF_CUDA(cudaMemsetAsync(A->loss, 0, sizeof(double), st));
+        const double n4 = (double)N * N * (double)N * N;
+        for (int seg = 0; seg < A->nseg; ++seg) {
+            const int t0 = seg * A->K, t1 = std::min(A->nsteps, t0 + A->K);
+            AdjRecord rec{nullptr, nullptr, A->window > 0 ? A->loss : nullptr, A->nsteps - A->window - t0,
+                          1.0 / ((double)(A->window > 0 ? A->window : 1) * n4)};
+            QAF_TRY((OpRecord::run<real, N>(m, &A->p, t1 - t0, &rec, st)));
+            if (t1 < A->nsteps) {
+                unsigned char* c = A->ckpt + (size_t)(seg + 1) * 3 * ns * cb;
+                void* dst[3] = {adj_field<real>(c, ns, 0), adj_field<real>(c, ns, 1), adj_field<real>(c, ns, 2)};
+                QAF_TRY((OpStore::run<real, N>(m, dst, st)));
+            }
+        }
+        if (sT[0] && sT[1] && sT[2]) QAF_TRY((OpStore::run<real, N>(m, sT, st)));
+        double h = 0;
+        QAF_CUDA(cudaMemcpyAsync(&h, A->loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+        QAF_CUDA(cudaStreamSynchronize(st));
+        if (loss) *loss = h;
+        return post_launch("qaf_adjoint_forward");
+    }
+};
+
+struct OpAdjBackward {
+    template <typename real, int N>
+    static qaf_status run(qaf_adjoint* A, const void* const* gT, double gloss, void* const* g0, void* galpha,
+                          cudaStream_t st) {
+        using C = Cfg<real, N>;
+        constexpr int H = N / 2;
+        constexpr int W = C::W, EC = C::EC, ER = C::ERT, ROWS = C::ROWS_T;
+        constexpr int COL_THREADS = W * (N / EC), ROW_THREADS = ROWS * (H / ER);
+        constexpr size_t COL_SMEM = (size_t)W * N * sizeof(cplx<real>);
+        constexpr size_t ROW_SMEM = (size_t)ROWS * (H * sizeof(cplx<real>) + (size_t)NGA * N * sizeof(real));
+        static bool attrs = false;
+        if (!attrs) {
+            QAF_CUDA(cudaFuncSetAttribute(adj_col_kernel<real, N, W, EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COL_SMEM));
+            QAF_CUDA(cudaFuncSetAttribute(adj_row_kernel<real, N, ER, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROW_SMEM));
+            attrs = true;
+        }
+        qaf_mesh* m = A->m;
+        const size_t ns = A->ns, cb = sizeof(cplx<real>);
+        const size_t slot = (size_t)PF_COUNT * N * N;
+        QAF_TRY(ensure_ws<real>(m));
+        QAF_TRY(ensure_if<real>(m, &A->p, st));
+        Workspace<real>& w = ws<real>(m);
+
+        AdjArgs<real> a;
+        std::memset(&a, 0, sizeof(a));
+        a.dkx = (real)m->dkx; a.dky = (real)m->dky; a.dt = (real)A->p.dt; a.lambda = (real)A->p.lambda;
+        a.ce = (real)(1.0 / (A->p.er * A->p.re));
+        a.advect = A->p.advect_omega ? 1 : 0;
+        a.kx_keep = (H + 1 - 1) * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
+        a.tw = w.tw; a.ex = w.ex; a.ey = w.ey;
+        for (int c = 0; c < 4; ++c) a.e0[c] = w.e0[c];
+        a.Tg = reinterpret_cast<cplx<real>*>(A->Tg); a.Tx = reinterpret_cast<cplx<real>*>(A->Tx);
+        for (int f = 0; f < 3; ++f) {
+            a.abar[f] = adj_field<real>(A->abar, ns, f);
+            a.sacc[f] = adj_field<real>(A->sacc, ns, f);
+            a.sbar[f] = adj_field<real>(A->sbar, ns, f);
+        }
+        a.edge = reinterpret_cast<cplx<real>*>(A->edge);
+        a.alpha_field = reinterpret_cast<const real*>(A->p.alpha_field);
+        a.alpha = (real)A->p.alpha;
+        a.alpha_grad = reinterpret_cast<real*>(A->agrad);
+        const real lw = (real)(A->window > 0 ? gloss / A->window : 0.0);
+        a.loss_w = lw;
+
+        for (int f = 0; f < 3; ++f) {
+            if (gT[f]) QAF_CUDA(cudaMemcpyAsync(a.sbar[f], gT[f], ns * cb, cudaMemcpyDeviceToDevice, st));
+            else QAF_CUDA(cudaMemsetAsync(a.sbar[f], 0, ns * cb, st));
+        }
+        QAF_CUDA(cudaMemsetAsync(A->agrad, 0, (size_t)N * N * sizeof(real), st));
+        const int T = A->nsteps;
+        auto in_window = [&](int n) { return A->window > 0 && gloss != 0.0 && n >= T - A->window + 1; };
+        auto col = [&]() {
+            adj_col_kernel<real, N, W, EC><<<H / W + 1, COL_THREADS, COL_SMEM, st>>>(a);
+            m->launches += 1;
+        };
+        bool started = false;
+        for (int seg = A->nseg - 1; seg >= 0; --seg) {
+            const int t0 = seg * A->K, t1 = std::min(T, t0 + A->K);
+            unsigned char* c = A->ckpt + (size_t)seg * 3 * ns * cb;
+            const void* cs[3] = {adj_field<real>(c, ns, 0), adj_field<real>(c, ns, 1), adj_field<real>(c, ns, 2)};
+            QAF_TRY((OpLoad::run<real, N>(m, const_cast<void* const*>(cs), st)));
+            AdjRecord rec{A->phys, A->wlog, nullptr, 0, 0.0};
+            QAF_TRY((OpRecord::run<real, N>(m, &A->p, t1 - t0, &rec, st)));
+            auto w_at = [&](int n) -> const cplx<real>* {   // w of the state at time n (t0 <= n <= t1)
+                if (n == t0) return adj_field<real>(c, ns, 0);
+                return reinterpret_cast<const cplx<real>*>(A->wlog) + (size_t)(n - 1 - t0) * ns;
+            };
+            for (int n = t1 - 1; n >= t0; --n) {
+                if (!started) {
+                    a.stage = 0; a.emit = 1;
+                    a.wstate = in_window(T) ? w_at(T) : nullptr;
+                    col();
+                    started = true;
+                }
+                for (int s = 4; s >= 1; --s) {
+                    a.phys = reinterpret_cast<const real*>(A->phys) + ((size_t)(n - t0) * 4 + (s - 1)) * slot;
+                    adj_row_kernel<real, N, ER, ROWS><<<N / ROWS, ROW_THREADS, ROW_SMEM, st>>>(a);
+                    m->launches += 1;
+                    a.stage = s;
+                    a.emit = (s > 1 || n > 0) ? 1 : 0;
+                    a.wstate = (s == 1 && in_window(n)) ? w_at(n) : nullptr;
+                    col();
+                }
+            }
+        }
+        for (int f = 0; f < 3; ++f)
+            if (g0[f]) QAF_CUDA(cudaMemcpyAsync(g0[f], a.sbar[f], ns * cb, cudaMemcpyDeviceToDevice, st));
+        if (galpha)
+            QAF_CUDA(cudaMemcpyAsync(galpha, A->agrad, (size_t)N * N * sizeof(real), cudaMemcpyDeviceToDevice, st));
+        return post_launch("qaf_adjoint_backward");
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+qaf_status qaf_adjoint_create(qaf_mesh* m, int nsteps, int checkpoint_every, int loss_window, qaf_adjoint** out) {
+    QAF_TRY(check_mesh(m));
+    if (!out) return fail(QAF_ERR_INVALID, "null output");
+    *out = nullptr;
+    if (nsteps < 1) return fail(QAF_ERR_INVALID, "nsteps must be >= 1");
+    if (checkpoint_every < 1) return fail(QAF_ERR_INVALID, "checkpoint_every must be >= 1");
+    if (loss_window < 0 || loss_window > nsteps) return fail(QAF_ERR_INVALID, "loss_window must be in [0, nsteps]");
+    if (!qaf_supported(m->desc.nx, m->desc.dtype) || m->desc.nx != m->desc.ny)
+        return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size");
+    qaf_adjoint* A = new qaf_adjoint();
+    A->m = m;
+    A->nsteps = nsteps;
+    A->K = std::min(checkpoint_every, nsteps);
+    A->window = loss_window;
+    A->nseg = (nsteps + A->K - 1) / A->K;
+    const int N = m->desc.nx;
+    A->ns = spec_elems(m);
+    A->np = phys_elems(m);
+    A->rb = real_bytes(m);
+    const size_t cb = 2 * A->rb;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    const size_t o_ck = take((size_t)A->nseg * 3 * A->ns * cb);
+    const size_t o_wl = take((size_t)A->K * A->ns * cb);
+    const size_t o_ph = take((size_t)A->K * 4 * PF_COUNT * A->np * A->rb);
+    const size_t o_tg = take((size_t)NGA * N * (N / 2) * cb);
+    const size_t o_tx = take((size_t)PF_COUNT * N * (N / 2) * cb);
+    const size_t o_ab = take(3 * A->ns * cb), o_sa = take(3 * A->ns * cb), o_sb = take(3 * A->ns * cb);
+    const size_t o_ed = take(6 * (size_t)N * cb);
+    const size_t o_ag = take(A->np * A->rb);
+    const size_t o_ls = take(sizeof(double));
+    cudaError_t e = cudaMalloc((void**)&A->blk, off);
+    if (e != cudaSuccess) {
+        delete A;
+        return fail(QAF_ERR_ALLOC, std::string("qaf_adjoint_create: cudaMalloc of ") + std::to_string(off >> 20) +
+                                       " MiB: " + cudaGetErrorString(e));
+    }
+    A->ckpt = A->blk + o_ck; A->wlog = A->blk + o_wl; A->phys = A->blk + o_ph; A->Tg = A->blk + o_tg;
+    A->Tx = A->blk + o_tx; A->abar = A->blk + o_ab; A->sacc = A->blk + o_sa; A->sbar = A->blk + o_sb;
+    A->edge = A->blk + o_ed; A->agrad = A->blk + o_ag; A->loss = reinterpret_cast<double*>(A->blk + o_ls);
+    *out = A;
+    return QAF_OK;
+}
+
+qaf_status qaf_adjoint_destroy(qaf_adjoint* A) {
+    if (!A) return QAF_OK;
+    if (A->blk) cudaFree(A->blk);
+    delete A;
+    return QAF_OK;
+}
+
+qaf_status qaf_adjoint_forward(qaf_adjoint* A, const qaf_params* p, const void* w0, const void* r1_0, const void* r2_0,
+                               void* wT, void* r1T, void* r2T, double* loss, void* stream) {
+    if (!A) return fail(QAF_ERR_INVALID, "null adjoint");
+    QAF_TRY(check_params(p));
+    if (!w0 || !r1_0 || !r2_0) return fail(QAF_ERR_INVALID, "null initial state");
+    A->p = *p;
+    A->have_forward = false;
+    const void* s0[3] = {w0, r1_0, r2_0};
+    void* sT[3] = {wT, r1T, r2T};
+    QAF_TRY(dispatch<OpAdjForward>(A->m, A, (const void* const*)s0, (void* const*)sT, loss, (cudaStream_t)stream));
+    A->have_forward = true;
+    return QAF_OK;
+}
+
+qaf_status qaf_adjoint_backward(qaf_adjoint* A, const void* gwT, const void* gr1T, const void* gr2T, double gloss,
+                                void* gw0, void* gr1_0, void* gr2_0, void* galpha, void* stream) {
+    if (!A) return fail(QAF_ERR_INVALID, "null adjoint");
+    if (!A->have_forward) return fail(QAF_ERR_INVALID, "qaf_adjoint_backward needs a qaf_adjoint_forward first");
+    if (!std::isfinite(gloss)) return fail(QAF_ERR_INVALID, "non-finite loss gradient");
+    const void* gT[3] = {gwT, gr1T, gr2T};
+    void* g0[3] = {gw0, gr1_0, gr2_0};
+    return dispatch<OpAdjBackward>(A->m, A, (const void* const*)gT, gloss, (void* const*)g0, galpha,
+                                   (cudaStream_t)stream);
+}
+
+}  // extern "C"
+

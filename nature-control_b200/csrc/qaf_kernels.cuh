@@ -688,9 +688,9 @@ struct RowKernel {
             const real p12 = sg2 + (2 * L1 * r2 - 2 * r1 * L2) - al * r2;
             kp(4, e) = sg2 + (2 * L2 * r1 - 2 * r2 * L1) - al * r2;
             v[e] = mk<real>(p11, p12);
-            if (a.phys_out) kp(3, e) = S;
+            if (a.phys_out && a.phys_all) kp(3, e) = S;
         }
-        if (a.phys_out) { dump_slot(9, 3); dump(10, v, false); dump(11, v, true); dump_slot(12, 4); }
+        if (a.phys_out && a.phys_all) { dump_slot(9, 3); dump(10, v, false); dump(11, v, true); dump_slot(12, 4); }
         {
             cplx<real>* g0 = grow(0); cplx<real>* g1 = grow(1);
             r2c(v, 1, 2, g0v, g1v, [=](int k, cplx<real> P, cplx<real> Q, cplx<real>, cplx<real>) {

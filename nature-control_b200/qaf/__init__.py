@@ -38,7 +38,8 @@ EXPORTS = [
     "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_state_advance_timed", "qaf_launch_count",
     "qaf_init_random_q", "qaf_step_noalloc", "qaf_ensemble_create", "qaf_ensemble_destroy",
     "qaf_ensemble_init_random", "qaf_ensemble_load", "qaf_ensemble_store", "qaf_ensemble_advance",
-    "qaf_ensemble_diagnostics", "qaf_ensemble_set_controls",
+    "qaf_ensemble_diagnostics", "qaf_ensemble_set_controls", "qaf_adjoint_create", "qaf_adjoint_destroy",
+    "qaf_adjoint_forward", "qaf_adjoint_backward",
 ]
 
 
@@ -137,6 +138,10 @@ def lib():
         L.qaf_ensemble_advance.argtypes = [vp, cp, vp]
         L.qaf_ensemble_diagnostics.argtypes = [vp, dp, vp]
         L.qaf_ensemble_set_controls.argtypes = [vp, dp, dp, vp]
+        L.qaf_adjoint_create.argtypes = [vp, cp, cp, cp, ctypes.POINTER(vp)]
+        L.qaf_adjoint_destroy.argtypes = [vp]
+        L.qaf_adjoint_forward.argtypes = [vp, ctypes.POINTER(CParams), vp, vp, vp, vp, vp, vp, dp, vp]
+        L.qaf_adjoint_backward.argtypes = [vp, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -436,4 +441,53 @@ class Ensemble:
         out = (ctypes.c_double * (2 * k))()
         _check(lib().qaf_ensemble_diagnostics(self._h, out, _stream()))
         return [(out[2 * i], out[2 * i + 1]) for i in range(k)]
+
+
+class Adjoint:
+    """Reverse-mode gradients of `nsteps` IF-RK4 steps on `mesh` (include/qaf.h,
+    qaf_adjoint_*): of the mean enstrophy of the states after the last
+    `loss_window` steps and of any function of the final state, with respect
+    to the initial spectra and the activity field Ra(x). The state is kept
+    every `checkpoint_every` steps and each segment is recomputed once during
+    the backward sweep. The mesh's resident state is overwritten."""
+
+    def __init__(self, mesh: Mesh, nsteps: int, checkpoint_every: int = 64, loss_window: int = 0):
+        self.mesh, self.nsteps, self.K, self.window = mesh, nsteps, checkpoint_every, loss_window
+        h = ctypes.c_void_p()
+        _check(lib().qaf_adjoint_create(mesh._h, nsteps, checkpoint_every, loss_window, ctypes.byref(h)))
+        self._h = h
+        self._alpha = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.qaf_adjoint_destroy(h)
+            self._h = None
+
+    def forward(self, p: Params, w0, r1_0, r2_0, final_state: bool = True):
+        """Run the steps; returns (loss, (wT, r1T, r2T) or None)."""
+        m = self.mesh
+        self._alpha = p.alpha_field          # must outlive the backward call
+        cp = p.c()
+        out = (m.new_spec(), m.new_spec(), m.new_spec()) if final_state else None
+        ptrs = [m._chk_spec(t) for t in out] if out else [None, None, None]
+        loss = ctypes.c_double()
+        _check(lib().qaf_adjoint_forward(self._h, ctypes.byref(cp), m._chk_spec(w0), m._chk_spec(r1_0),
+                                         m._chk_spec(r2_0), *ptrs, ctypes.byref(loss), _stream()))
+        return loss.value, out
+
+    def backward(self, grad_final=None, grad_loss: float = 1.0, want_alpha: bool = True):
+        """Gradients (gw0, gr1_0, gr2_0, galpha) given dL/d(final state) (or None) and dL/d(loss)."""
+        m = self.mesh
+        g = [None, None, None]
+        keep = []
+        if grad_final is not None:
+            keep = [t.contiguous() if t is not None else None for t in grad_final]
+            g = [m._chk_spec(t) if t is not None else None for t in keep]
+        gw, g1, g2 = m.new_spec(), m.new_spec(), m.new_spec()
+        ga = m.new_phys() if want_alpha else None
+        _check(lib().qaf_adjoint_backward(self._h, *g, float(grad_loss), m._chk_spec(gw), m._chk_spec(g1),
+                                          m._chk_spec(g2), m._chk_phys(ga) if ga is not None else None,
+                                          _stream()))
+        return gw, g1, g2, ga
 

@@ -58,6 +58,7 @@ def lib():
         for name in ("oracle_xderiv", "oracle_yderiv", "oracle_laplacian"):
             getattr(L, name).argtypes = [pp, dp, dp]
         L.oracle_vel.argtypes = [pp, dp, dp, dp]
+        L.oracle_step_tlm.argtypes = [pp, dp, dp, dp, dp, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, dp, dp]
         L.oracle_dealias.argtypes = [pp, dp]
         L.oracle_if_tables.argtypes = [pp, ctypes.c_int, ctypes.c_double, dp, dp]
         L.oracle_nonlinear.argtypes = [pp, dp, dp, dp, dp, dp, dp, dp, dp]
@@ -169,6 +170,20 @@ def step(p, w, r1, r2, nsteps, integrator=IFRK4, alpha_field=None):
     af = None if alpha_field is None else np.ascontiguousarray(alpha_field, dtype=np.float64)
     _check(lib().oracle_step(ctypes.byref(p), integrator, _p(af), _p(w), _p(r1), _p(r2), nsteps))
     return w, r1, r2
+
+
+def step_tlm(p, w, r1, r2, dw, dr1, dr2, nsteps, loss_window, alpha_field=None, dalpha_field=None):
+    """IF-RK4 with its tangent-linear model: returns (final state, final tangent,
+    loss, dloss), loss the mean enstrophy 0.5 mean(w^2) of the states after the
+    last ``loss_window`` steps and dloss its derivative along the tangent."""
+    w, r1, r2 = _spec(w).copy(), _spec(r1).copy(), _spec(r2).copy()
+    dw, dr1, dr2 = _spec(dw).copy(), _spec(dr1).copy(), _spec(dr2).copy()
+    af = None if alpha_field is None else np.ascontiguousarray(alpha_field, dtype=np.float64)
+    daf = None if dalpha_field is None else np.ascontiguousarray(dalpha_field, dtype=np.float64)
+    loss, dloss = ctypes.c_double(), ctypes.c_double()
+    _check(lib().oracle_step_tlm(ctypes.byref(p), _p(af), _p(daf), _p(w), _p(r1), _p(r2), _p(dw), _p(dr1), _p(dr2),
+                                 nsteps, loss_window, ctypes.byref(loss), ctypes.byref(dloss)))
+    return (w, r1, r2), (dw, dr1, dr2), loss.value, dloss.value
 
 
 def diagnostics(p, w, nshells=0):

@@ -485,6 +485,120 @@ bool valid(const oracle_params* p) {
 
 } // namespace
 
+// ---------------------------------------------------------------------------
+// Tangent-linear model of the nonlinear terms: the derivative of
+// all_nonlinear along (dw, dr1, dr2, dRa), operation by operation in the same
+// sequence (every transform and multiplier is linear; the products take the
+// product rule). W holds the forward evaluation at the same stage input
+// (all_nonlinear already run on it); D.{w,r1,r2}curr.spec hold the tangent
+// input and D.Ra the tangent activity; the tangent terms land in
+// D.{w,r1,r2}nonl.spec.
+// ---------------------------------------------------------------------------
+void all_nonlinear_tlm(Ctx& c, Work& W, Work& D) {
+    const double lambda = c.p->lambda;
+    const size_t np = c.m.np(), ns = c.m.ns();
+    // forward fields the products need besides W's current ones
+    Field L1(c.m), L2(c.m), ux(c.m), sh(c.m), t1(c.m), t2(c.m);
+    c.Laplacian(L1.spec, W.r1curr.spec); c.Bwd(L1.phys, L1.spec);
+    c.Laplacian(L2.spec, W.r2curr.spec); c.Bwd(L2.phys, L2.spec);
+    c.xDeriv(ux.spec, W.u.spec); c.Bwd(ux.phys, ux.spec);
+    c.yDeriv(t1.spec, W.u.spec); c.xDeriv(t2.spec, W.v.spec);
+    for (size_t k = 0; k < ns; ++k) sh.spec[k] = t1.spec[k] + t2.spec[k];
+    c.Bwd(sh.phys, sh.spec);
+    const auto& w = W.wcurr.phys; const auto& r1 = W.r1curr.phys; const auto& r2 = W.r2curr.phys;
+    const auto& u = W.u.phys; const auto& v = W.v.phys; const auto& S = W.S.phys;
+    // tangent curr_func
+    c.Bwd(D.r1curr.phys, D.r1curr.spec);
+    c.Bwd(D.r2curr.phys, D.r2curr.spec);
+    c.Bwd(D.wcurr.phys, D.wcurr.spec);
+    for (size_t k = 0; k < np; ++k)
+        D.S.phys[k] = S[k] > 0 ? 4.0 * (r1[k] * D.r1curr.phys[k] + r2[k] * D.r2curr.phys[k]) / S[k] : 0.0;
+    c.vel(D.wcurr.spec, D.u.spec, D.v.spec);
+    c.Bwd(D.u.phys, D.u.spec);
+    c.Bwd(D.v.phys, D.v.spec);
+    const auto& dw = D.wcurr.phys; const auto& dr1 = D.r1curr.phys; const auto& dr2 = D.r2curr.phys;
+    const auto& du = D.u.phys; const auto& dv = D.v.phys; const auto& dS = D.S.phys;
+    Field dL1(c.m), dL2(c.m), dux(c.m), dsh(c.m);
+    c.Laplacian(dL1.spec, D.r1curr.spec); c.Bwd(dL1.phys, dL1.spec);
+    c.Laplacian(dL2.spec, D.r2curr.spec); c.Bwd(dL2.phys, dL2.spec);
+    c.xDeriv(dux.spec, D.u.spec); c.Bwd(dux.phys, dux.spec);
+    c.yDeriv(t1.spec, D.u.spec); c.xDeriv(t2.spec, D.v.spec);
+    for (size_t k = 0; k < ns; ++k) dsh.spec[k] = t1.spec[k] + t2.spec[k];
+    c.Bwd(dsh.phys, dsh.spec);
+
+    // wnonl_func
+    if (c.p->advect_omega) {
+        for (size_t k = 0; k < np; ++k) D.wnonl.phys[k] = -(du[k] * w[k] + u[k] * dw[k]);
+        c.Fwd(D.wnonl.spec, D.wnonl.phys);
+        c.xDeriv(D.wnonl.spec, D.wnonl.spec);
+        c.Bwd(D.wnonl.phys, D.wnonl.spec);
+        for (size_t k = 0; k < np; ++k) D.aux.phys[k] = -(dv[k] * w[k] + v[k] * dw[k]);
+        c.Fwd(D.aux.spec, D.aux.phys);
+        c.yDeriv(D.aux.spec, D.aux.spec);
+        c.Bwd(D.aux.phys, D.aux.spec);
+        for (size_t k = 0; k < np; ++k) D.wnonl.phys[k] = D.wnonl.phys[k] + D.aux.phys[k];
+    } else {
+        for (size_t k = 0; k < np; ++k) D.wnonl.phys[k] = 0.0;
+    }
+    c.Fwd(D.wnonl.spec, D.wnonl.phys);
+    // single: -lambda S L + lambda S (S^2 - 1) r; Rar: -Ra r; cross: 2 La b - 2 a Lb
+    auto dsingle = [&](size_t k, double L, double dL, double r, double dr) {
+        return -lambda * (dS[k] * L + S[k] * dL) + lambda * (3.0 * S[k] * S[k] - 1.0) * dS[k] * r +
+               lambda * S[k] * (S[k] * S[k] - 1.0) * dr;
+    };
+    for (size_t k = 0; k < np; ++k) {
+        const double dcross12 = 2.0 * (dL1.phys[k] * r2[k] + L1.phys[k] * dr2[k]) - 2.0 * (dr1[k] * L2.phys[k] + r1[k] * dL2.phys[k]);
+        D.p11.phys[k] = dsingle(k, L1.phys[k], dL1.phys[k], r1[k], dr1[k]) - (D.Ra[k] * r1[k] + W.Ra[k] * dr1[k]);
+        D.p12.phys[k] = dsingle(k, L2.phys[k], dL2.phys[k], r2[k], dr2[k]) + dcross12 - (D.Ra[k] * r2[k] + W.Ra[k] * dr2[k]);
+        D.p21.phys[k] = dsingle(k, L2.phys[k], dL2.phys[k], r2[k], dr2[k]) - dcross12 - (D.Ra[k] * r2[k] + W.Ra[k] * dr2[k]);
+    }
+    c.Fwd(D.p11.spec, D.p11.phys);
+    c.Fwd(D.p12.spec, D.p12.phys);
+    c.Fwd(D.p21.spec, D.p21.phys);
+    const double ce = 1.0 / (c.p->er * c.p->re);
+    for (size_t k = 0; k < ns; ++k) {
+        const double kx = c.m.kx[k], ky = c.m.ky[k];
+        D.wnonl.spec[k] = D.wnonl.spec[k] + ce * (-1.0 * kx * kx * D.p12.spec[k] + 2.0 * kx * ky * D.p11.spec[k]
+                                                  + ky * ky * D.p21.spec[k]);
+    }
+    // r1nonl_func, r2nonl_func
+    for (int f = 0; f < 2; ++f) {
+        const auto& ra = f == 0 ? r1 : r2;   // the field advanced
+        const auto& dra = f == 0 ? dr1 : dr2;
+        Field& out = f == 0 ? D.r1nonl : D.r2nonl;
+        for (size_t k = 0; k < np; ++k) {
+            const double rot = f == 0 ? -(dw[k] * r2[k] + w[k] * dr2[k]) : (dw[k] * r1[k] + w[k] * dr1[k]);
+            out.phys[k] = rot - (2.0 * S[k] * dS[k] * ra[k] + S[k] * S[k] * dra[k]);
+        }
+        c.Fwd(out.spec, out.phys);
+        for (size_t k = 0; k < np; ++k) D.aux.phys[k] = -(du[k] * ra[k] + u[k] * dra[k]);
+        c.Fwd(D.aux.spec, D.aux.phys);
+        c.xDeriv(D.aux.spec, D.aux.spec);
+        for (size_t k = 0; k < np; ++k) D.aux1.phys[k] = -(dv[k] * ra[k] + v[k] * dra[k]);
+        c.Fwd(D.aux1.spec, D.aux1.phys);
+        c.yDeriv(D.aux1.spec, D.aux1.spec);
+        for (size_t k = 0; k < ns; ++k) out.spec[k] = out.spec[k] + (D.aux.spec[k] + D.aux1.spec[k]);
+        for (size_t k = 0; k < np; ++k)
+            D.aux.phys[k] = f == 0 ? lambda * (dS[k] * ux.phys[k] + S[k] * dux.phys[k])
+                                   : 0.5 * lambda * (dS[k] * sh.phys[k] + S[k] * dsh.phys[k]);
+        c.Fwd(D.aux.spec, D.aux.phys);
+        for (size_t k = 0; k < ns; ++k) out.spec[k] = out.spec[k] + D.aux.spec[k];
+    }
+}
+
+// enstrophy 0.5 mean(w^2) of a spectral vorticity and its derivative along dw
+void enstrophy_tlm(Ctx& c, const cplx* ws, const cplx* dws, double* z, double* dz) {
+    const size_t ns = c.m.ns(), np = c.m.np();
+    std::vector<cplx> a(ws, ws + ns), b(dws, dws + ns);
+    std::vector<double> wp(np), dwp(np);
+    bwd2d(c.m.nx, c.m.ny, a.data(), wp.data());
+    bwd2d(c.m.nx, c.m.ny, b.data(), dwp.data());
+    double s = 0, ds = 0;
+    for (size_t k = 0; k < np; ++k) { s += wp[k] * wp[k]; ds += wp[k] * dwp[k]; }
+    *z = 0.5 * s / (double)np;
+    *dz = ds / (double)np;
+}
+
 extern "C" {
 
 int oracle_tables(const oracle_params* p, double* kx, double* ky, double* k2, double* cutoff) {
@@ -726,6 +840,94 @@ int oracle_diagnostics(const oracle_params* p, const double* w, double* energy, 
 void oracle_random_q_init(unsigned long long seed, int nx, int ny, double lo, double hi, double* w, double* r1,
                           double* r2) {
     qaf_random_q_init(seed, nx, ny, lo, hi, w, r1, r2);
+}
+
+
+// IF-RK4 (friction.cu:212-259) advanced together with its tangent-linear model.
+int oracle_step_tlm(const oracle_params* p, const double* alpha_field, const double* dalpha_field, double* w,
+                    double* r1, double* r2, double* dw, double* dr1, double* dr2, int nsteps, int loss_window,
+                    double* loss, double* dloss) {
+    if (!valid(p) || nsteps < 0 || loss_window < 0 || loss_window > nsteps) return 1;
+    Ctx c(p);
+    Work W(c.m), D(c.m);
+    set_ra(c, W, alpha_field);
+    for (size_t k = 0; k < c.m.np(); ++k) D.Ra[k] = dalpha_field ? dalpha_field[k] : 0.0;
+    const size_t ns = c.m.ns();
+    const double dt = p->dt;
+    std::vector<double> IFw, IFwh, IFq, IFqh;
+    if_tables(c, 0, dt, IFw, IFwh);
+    if_tables(c, 1, dt, IFq, IFqh);
+    cplx* old[3] = {as_cplx(w), as_cplx(r1), as_cplx(r2)};
+    cplx* dold[3] = {as_cplx(dw), as_cplx(dr1), as_cplx(dr2)};
+    std::vector<cplx>* curr[3] = {&W.wcurr.spec, &W.r1curr.spec, &W.r2curr.spec};
+    std::vector<cplx>* dcurr[3] = {&D.wcurr.spec, &D.r1curr.spec, &D.r2curr.spec};
+    std::vector<cplx>* nonl[3] = {&W.wnonl.spec, &W.r1nonl.spec, &W.r2nonl.spec};
+    std::vector<cplx>* dnonl[3] = {&D.wnonl.spec, &D.r1nonl.spec, &D.r2nonl.spec};
+    std::vector<cplx> nw[3] = {std::vector<cplx>(ns), std::vector<cplx>(ns), std::vector<cplx>(ns)};
+    std::vector<cplx> dnw[3] = {std::vector<cplx>(ns), std::vector<cplx>(ns), std::vector<cplx>(ns)};
+    const std::vector<double>* E[3] = {&IFw, &IFq, &IFq};
+    const std::vector<double>* Eh[3] = {&IFwh, &IFqh, &IFqh};
+    auto eval = [&]() {
+        // the forward's Bwd may symmetrise curr in place; evaluate the tangent on the same inputs
+        all_nonlinear(c, W);
+        all_nonlinear_tlm(c, W, D);
+    };
+    double L = 0, dL = 0;
+    for (int s = 0; s < nsteps; ++s) {
+        for (int f = 0; f < 3; ++f)
+            for (size_t k = 0; k < ns; ++k) {
+                nw[f][k] = old[f][k] * (*E[f])[k]; (*curr[f])[k] = old[f][k];
+                dnw[f][k] = dold[f][k] * (*E[f])[k]; (*dcurr[f])[k] = dold[f][k];
+            }
+        eval();
+        for (int f = 0; f < 3; ++f)
+            for (size_t k = 0; k < ns; ++k) {
+                cplx an = (*nonl[f])[k] * dt, dan = (*dnonl[f])[k] * dt;
+                nw[f][k] = nw[f][k] + 1.0 / 6.0 * ((*E[f])[k]) * an;
+                dnw[f][k] = dnw[f][k] + 1.0 / 6.0 * ((*E[f])[k]) * dan;
+                (*curr[f])[k] = (old[f][k] + an / 2.0) * ((*Eh[f])[k]);
+                (*dcurr[f])[k] = (dold[f][k] + dan / 2.0) * ((*Eh[f])[k]);
+            }
+        eval();
+        for (int f = 0; f < 3; ++f)
+            for (size_t k = 0; k < ns; ++k) {
+                cplx bn = (*nonl[f])[k] * dt, dbn = (*dnonl[f])[k] * dt;
+                nw[f][k] = nw[f][k] + 1.0 / 3.0 * (*Eh[f])[k] * bn;
+                dnw[f][k] = dnw[f][k] + 1.0 / 3.0 * (*Eh[f])[k] * dbn;
+                (*curr[f])[k] = old[f][k] * ((*Eh[f])[k]) + bn / 2.0;
+                (*dcurr[f])[k] = dold[f][k] * ((*Eh[f])[k]) + dbn / 2.0;
+            }
+        eval();
+        for (int f = 0; f < 3; ++f)
+            for (size_t k = 0; k < ns; ++k) {
+                cplx cn = (*nonl[f])[k] * dt, dcn = (*dnonl[f])[k] * dt;
+                nw[f][k] = nw[f][k] + 1.0 / 3.0 * (*Eh[f])[k] * cn;
+                dnw[f][k] = dnw[f][k] + 1.0 / 3.0 * (*Eh[f])[k] * dcn;
+                (*curr[f])[k] = old[f][k] * (*E[f])[k] + cn * (*Eh[f])[k];
+                (*dcurr[f])[k] = dold[f][k] * (*E[f])[k] + dcn * (*Eh[f])[k];
+            }
+        eval();
+        for (int f = 0; f < 3; ++f)
+            for (size_t k = 0; k < ns; ++k) {
+                cplx dn = (*nonl[f])[k] * dt, ddn = (*dnonl[f])[k] * dt;
+                nw[f][k] = nw[f][k] + 1.0 / 6.0 * dn;
+                dnw[f][k] = dnw[f][k] + 1.0 / 6.0 * ddn;
+            }
+        for (int f = 0; f < 3; ++f)
+            for (size_t k = 0; k < ns; ++k) {
+                old[f][k] = nw[f][k] * c.m.cutoff[k];
+                dold[f][k] = dnw[f][k] * c.m.cutoff[k];
+            }
+        if (s >= nsteps - loss_window) {
+            double z, dz;
+            enstrophy_tlm(c, old[0], dold[0], &z, &dz);
+            L += z / loss_window;
+            dL += dz / loss_window;
+        }
+    }
+    if (loss) *loss = L;
+    if (dloss) *dloss = dL;
+    return 0;
 }
 
 } // extern "C"

@@ -86,6 +86,15 @@ int oracle_step(const oracle_params* p, int integrator, const double* alpha_fiel
 int oracle_diagnostics(const oracle_params* p, const double* w, double* energy,
                        double* enstrophy, double* spectrum, int nshells);
 
+/* IF-RK4 steps with the tangent-linear model (the reference gradient of the
+ * discrete adjoint): (w, r1, r2) advance as in oracle_step and (dw, dr1, dr2)
+ * as their derivative along the initial tangent and the activity tangent
+ * dalpha_field (NULL: zero). loss = mean enstrophy (0.5 mean(w^2)) of the
+ * states after the last loss_window steps, dloss its directional derivative. */
+int oracle_step_tlm(const oracle_params* p, const double* alpha_field, const double* dalpha_field,
+                    double* w, double* r1, double* r2, double* dw, double* dr1, double* dr2,
+                    int nsteps, int loss_window, double* loss, double* dloss);
+
 /* the seeded random-Q initial state of include/qaf_init.h (for checking the
  * numpy restatement of the generator) */
 void oracle_random_q_init(unsigned long long seed, int nx, int ny, double lo, double hi,
