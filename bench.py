@@ -1,7 +1,7 @@
 """Throughput benchmark of the IF-RK4 pseudo-spectral step (w, r1, r2).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl qaf|reference] [--dtype f32|f64]
-                    [--workload plain|ensemble]
+                    [--workload plain|ensemble|adjoint]
 
 Workload: the "plain throughput" configuration — 1024 x 1024 periodic grid,
 L = 16 pi, friction solver parameters Re = 1 (nu = 1), Rf = 0.1 (mu = 0.1),
@@ -31,6 +31,15 @@ other parameters as above; metric sum_i N_i^2 * steps / s. `value` is the
 batched stepper (one CUDA graph per step); `looped` is the plain solver
 looped over the same instances. Under torchrun the instances are sharded
 over ranks (strong scaling, no exchange while stepping).
+
+--workload adjoint: 256 x 256, FP32, 2000 IF-RK4 steps dt = 1e-3, activity
+Ra(x) = 1 + 0.1 * (unit-variance Gaussian-smoothed N(0,1) noise, width 4
+cells, seed 2), loss = mean enstrophy of the states after the last 100 steps,
+checkpoints every 64 steps. A bench step is one forward + backward pass of
+the whole horizon (--steps is capped at 5, 3 warm-up passes). `value` is
+(adjoint + recompute time) / (plain forward time); also reported: the
+directional derivatives of the FP32 and FP64 adjoint gradients against
+central differences of the FP64 forward on 16 random directions.
 """
 from __future__ import annotations
 
@@ -56,6 +65,8 @@ ENS_COUNT = 256
 ENS_SEED = 3
 ENS_DT = 1e-3
 ENS_METRIC = "sum_i N_i^2*steps/s, 256-instance mixed-size ensemble, IF-RK4"
+ADJ_N, ADJ_STEPS, ADJ_DT, ADJ_K, ADJ_WINDOW, ADJ_SEED = 256, 2000, 1e-3, 64, 100, 2
+ADJ_METRIC = "(adjoint + recompute) time / forward time, 256^2 FP32, 2000 IF-RK4 steps, K=64"
 
 
 def parse():
@@ -68,7 +79,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
-    ap.add_argument("--workload", choices=["plain", "ensemble"], default="plain")
+    ap.add_argument("--workload", choices=["plain", "ensemble", "adjoint"], default="plain")
+    ap.add_argument("--no-fd", action="store_true", help="adjoint workload: skip the finite-difference check")
     ap.add_argument("--instances", type=int, default=ENS_COUNT)
     return ap.parse_args()
 
@@ -495,19 +507,220 @@ def run_reference_ensemble(a):
     }
 
 
+def smoothed_alpha(n, seed, width=4.0):
+    """1 + 0.1 * (N(0,1) noise smoothed by a periodic Gaussian of `width` cells, rescaled to unit variance)."""
+    import numpy as np
+    g = np.random.default_rng(seed).standard_normal((n, n))
+    k = np.fft.fftfreq(n) * n
+    kk = k[:, None] ** 2 + k[None, :] ** 2
+    s = np.real(np.fft.ifft2(np.fft.fft2(g) * np.exp(-0.5 * (2 * np.pi * width / n) ** 2 * kk)))
+    return 1.0 + 0.1 * s / s.std()
+
+
+def run_adjoint(a, world, rank, local):
+    import numpy as np
+    import torch
+
+    import qaf
+    import qaf.autograd as QA
+
+    n, T, K, Wn, dt = ADJ_N, ADJ_STEPS, ADJ_K, ADJ_WINDOW, ADJ_DT
+    reps, warm = max(1, min(a.steps, 5)), 3
+    alpha_np = smoothed_alpha(n, ADJ_SEED)
+    base = dict(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=dt, q_lin=1.0, advect_omega=1)
+
+    def setup(dtype):
+        mesh = qaf.Mesh(n, lx=L, dtype=dtype)
+        p = qaf.Params(**base)
+        p.alpha_field = torch.as_tensor(alpha_np).to(device="cuda", dtype=mesh.real_dtype)
+        return mesh, p, mesh.random_q(SEED)
+
+    mesh, p, s0 = setup(qaf.F32)
+    adj = qaf.Adjoint(mesh, T, K, Wn)
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+
+    def plain_forward():
+        mesh.load(*s0)
+        mesh.advance(p, T)
+
+    def fwd_bwd():
+        adj.forward(p, *s0, final_state=False)
+        adj.backward(None, 1.0)
+
+    for _ in range(warm):
+        plain_forward()
+        fwd_bwd()
+    barrier(world)
+    t_plain, t_af, t_bw = [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(reps):
+            e0, e1 = ev()
+            e0.record(); plain_forward(); e1.record()
+            torch.cuda.synchronize()
+            t_plain.append(e0.elapsed_time(e1))
+            e0, e1 = ev()
+            e0.record(); adj.forward(p, *s0, final_state=False); e1.record()
+            torch.cuda.synchronize()
+            t_af.append(e0.elapsed_time(e1))
+            l0 = mesh.launch_count()
+            e0, e1 = ev()
+            e0.record(); adj.backward(None, 1.0); e1.record()
+            torch.cuda.synchronize()
+            t_bw.append(e0.elapsed_time(e1))
+            launches = mesh.launch_count() - l0
+    barrier(world)
+    tp = max_over_ranks(statistics.median(t_plain), world)
+    taf = max_over_ranks(statistics.median(t_af), world)
+    tbw = max_over_ranks(statistics.median(t_bw), world)
+    ratio = tbw / tp
+
+    # end to end through the autograd wrapper: host activity and initial state in, gradients out
+    host_alpha = torch.as_tensor(alpha_np, dtype=mesh.real_dtype).pin_memory()
+    host_s0 = [x.cpu().pin_memory() for x in s0]
+    host_ga = torch.empty((n, n), dtype=mesh.real_dtype).pin_memory()
+
+    def e2e_pass():
+        al = host_alpha.to("cuda", non_blocking=True).requires_grad_()
+        st = [h.to("cuda", non_blocking=True).requires_grad_() for h in host_s0]
+        loss, _, _, _ = QA.rollout(mesh, p, *st, al, nsteps=T, checkpoint_every=K, loss_window=Wn)
+        loss.backward()
+        host_ga.copy_(al.grad, non_blocking=True)
+        return float(loss.item())
+
+    e2e_pass()
+    e0, e1 = ev()
+    e0.record(); e2e_pass(); e1.record()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1), world)
+
+    # model bytes of one backward step: the recompute (4 stages x 55 arrays + 9 recorded real fields
+    # per stage) and the adjoint (column: 9 in + 11 out + 9 RK arrays; row: 11 in + 9 real fields +
+    # 9 out + the activity gradient read and written)
+    ca = (n // 2 + 1) * n * 2 * 4
+    pr = n * n * 4
+    bytes_step = 4 * (55 * ca + 9 * pr) + 4 * ((9 + 11 + 9) * ca + (11 + 9) * ca + (9 + 2) * pr)
+    peak, peak_kind = peaks()
+    achieved = bytes_step * T / (tbw * 1e-3) / 1e9
+
+    fd = None
+    if not a.no_fd and rank == 0:
+        fd = adjoint_fd_check(qaf, torch, np, n, T, K, Wn, dt, base, alpha_np, adj, p, s0)
+
+    line = {
+        "metric": ADJ_METRIC, "value": ratio, "unit": "x", "n_gpus": world, "steps": reps, "warmup": warm,
+        "ms_per_step": tbw, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded random Q ~ U(-0.01,0.01), w = 0; seeded smoothed activity field)",
+        "config": {"workload": f"adjoint {n}x{n} FP32, {T} IF-RK4 steps dt={dt}, Ra(x) = 1 + 0.1 smoothed N(0,1) "
+                               f"(width 4 cells, seed {ADJ_SEED}), loss = mean enstrophy of the last {Wn} states, "
+                               f"checkpoints every {K} steps", "grid": n, "horizon": T,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "working set of a segment's recording (~600 MB) larger than L2"},
+        "forward_ms": tp, "adjoint_forward_ms": taf, "backward_ms": tbw,
+        "ratio_forward_with_checkpoints_plus_backward": (taf + tbw) / tp,
+        "fd_check": fd,
+        "roofline": {"bound": "hbm", "kernel": "backward step (recompute + adjoint kernels)",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_step": bytes_step},
+        "e2e": {"value": t_e2e / tp, "unit": "x", "ms": t_e2e,
+                "h2d_bytes_per_step": n * n * 4 + 3 * ca, "d2h_bytes_per_step": n * n * 4 + 8},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = adjoint_cpu_baseline(n, dt, alpha_np)
+    return line
+
+
+def adjoint_fd_check(qaf, torch, np, n, T, K, Wn, dt, base, alpha_np, adj32, p32, s0_32):
+    """Directional derivatives of the FP32 and FP64 adjoint gradients against central
+    differences of the FP64 forward, along 16 random directions of (Ra(x), initial spectra)."""
+    mesh = qaf.Mesh(n, lx=L, dtype=qaf.F64)
+    p = qaf.Params(**base)
+    alpha = torch.as_tensor(alpha_np, dtype=torch.float64, device="cuda")
+    p.alpha_field = alpha
+    s0 = [x.to(torch.complex128) for x in s0_32]
+    adj = qaf.Adjoint(mesh, T, K, Wn)
+    loss0, _ = adj.forward(p, *s0, final_state=False)
+    g64 = adj.backward(None, 1.0)
+    adj32.forward(p32, *s0_32, final_state=False)
+    g32 = adj32.backward(None, 1.0)
+    rng = np.random.default_rng(7)
+    scale = float(max(x.abs().max().item() for x in s0[1:]))
+    err32, err64 = [], []
+    for _ in range(16):
+        da = torch.as_tensor(smoothed_alpha(n, int(rng.integers(1 << 30))) - 1.0, device="cuda") * 10.0
+        ds = [torch.complex(torch.as_tensor(rng.standard_normal(x.shape)), torch.as_tensor(rng.standard_normal(x.shape)))
+              .to("cuda") * scale for x in s0]
+        eps = 1e-5
+
+        def loss_at(sign):
+            q = qaf.Params(**base)
+            q.alpha_field = (alpha + sign * eps * da).contiguous()
+            return adj.forward(q, *[(x + sign * eps * d).contiguous() for x, d in zip(s0, ds)], final_state=False)[0]
+
+        fdv = (loss_at(1) - loss_at(-1)) / (2 * eps)
+
+        def dot(g):
+            v = float((g[3].double() * da).sum())
+            for gi, d in zip(g[:3], ds):
+                gi = gi.to(torch.complex128)
+                v += float((gi.real * d.real + gi.imag * d.imag).sum())
+            return v
+        err64.append(abs(dot(g64) - fdv) / abs(fdv))
+        err32.append(abs(dot(g32) - fdv) / abs(fdv))
+    return {"directions": 16, "eps": 1e-5, "loss": loss0,
+            "max_rel_err_fp64_adjoint": max(err64), "max_rel_err_fp32_adjoint": max(err32),
+            "median_rel_err_fp32_adjoint": statistics.median(err32),
+            "reference": "central differences of the FP64 forward on the GPU"}
+
+
+def adjoint_cpu_baseline(n, dt, alpha_np):
+    """The FP64 host oracle's tangent-linear step on a bounded sample, per forward step (the oracle has
+    no adjoint: one TLM pass gives one directional derivative)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    p = O.params(n=n, L=L, dt=dt)
+    s0 = O.initial_spectra(SEED, n)
+    z = [np.zeros_like(s0[0])] * 3
+    steps = 2
+    O.step(p, *s0, 1, alpha_field=alpha_np)
+    t0 = time.perf_counter()
+    O.step(p, *s0, steps, alpha_field=alpha_np)
+    tf = (time.perf_counter() - t0) / steps
+    t0 = time.perf_counter()
+    O.step_tlm(p, *s0, *z, steps, 0, alpha_field=alpha_np, dalpha_field=alpha_np)
+    tt = (time.perf_counter() - t0) / steps
+    cores = int(os.environ.get("QAF_ORACLE_THREADS", os.cpu_count() or 1))
+    return {"value": tt / tf, "unit": "x", "cores": cores, "kind": "port",
+            "sample": f"{steps} FP64 steps at {n}^2 with the host oracle: forward {tf*1e3:.1f} ms/step, forward + "
+                      f"tangent-linear {tt*1e3:.1f} ms/step (one directional derivative per pass)"}
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         # one rank runs the reference; under torchrun the others exit without work
         rank, local = int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
         if rank == 0:
-            line = run_reference_ensemble(a) if a.workload == "ensemble" else run_reference(a, 1, rank, local)
+            if a.workload == "ensemble":
+                line = run_reference_ensemble(a)
+            elif a.workload == "adjoint":
+                line = {"impl": "reference", "unavailable": "the reference computes no gradients (no adjoint or "
+                                                            "tangent model anywhere in it)"}
+            else:
+                line = run_reference(a, 1, rank, local)
             print(json.dumps(line), flush=True)
         return
     world, rank, local = dist_init()
     import torch
     torch.cuda.set_device(local)
-    line = run_ensemble(a, world, rank, local) if a.workload == "ensemble" else run_qaf(a, world, rank, local)
+    if a.workload == "ensemble":
+        line = run_ensemble(a, world, rank, local)
+    elif a.workload == "adjoint":
+        line = run_adjoint(a, world, rank, local)
+    else:
+        line = run_qaf(a, world, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
