@@ -87,6 +87,24 @@ __device__ __forceinline__ void adj_combine(int p, cplx<real> v, real kx, real k
     }
 }
 
+// field of the adjoint state that the transposed product p feeds (0 w, 1 r1, 2 r2)
+__host__ __device__ constexpr int adj_target(int p) {
+    return (p == PF_R1 || p == PF_LR1) ? 1 : ((p == PF_R2 || p == PF_LR2) ? 2 : 0);
+}
+
+// conj(multiplier) of the forward field p applied to the transform v of its adjoint
+template <typename real>
+__device__ __forceinline__ cplx<real> adj_cmult(int p, cplx<real> v, real kx, real ky, real ik2) {
+    switch (p) {
+        case PF_U: return cmul_mi(cscale(v, ky * ik2));
+        case PF_V: return cmul_i(cscale(v, kx * ik2));
+        case PF_UX: return cscale(v, -kx * ky * ik2);
+        case PF_SH: return cscale(v, (kx * kx - ky * ky) * ik2);
+        case PF_LR1: case PF_LR2: return cscale(v, -(kx * kx + ky * ky));
+        default: return v;   // PF_W, PF_R1, PF_R2
+    }
+}
+
 // conj(multiplier) that maps the nonlinear adjoint lambda of field f(q) to g_q's spectrum
 template <typename real>
 __device__ __forceinline__ cplx<real> adj_emit(int q, cplx<real> lw, cplx<real> l1, cplx<real> l2, real kx, real ky,
@@ -326,42 +344,206 @@ __global__ void __launch_bounds__(W * (N / E)) adj_col_kernel(const __grid_const
     }
 }
 
-// One team of H/E threads per physical row n (half-length real transforms):
-// 11 C2R of the g rows, the transposed products at each point, 9 R2C.
-template <typename real, int N, int E, int ROWS>
-__global__ void __launch_bounds__(ROWS * (N / 2 / E)) adj_row_kernel(const __grid_constant__ AdjArgs<real> a) {
-    constexpr int H = N / 2, TEAM = H / E;
+// Field-parallel column kernel (grids up to 256^2): one team of N/E threads
+// per (transform, kx-column) — NGA teams per column, W columns per CTA — so the
+// nine forward and eleven inverse y-FFTs of a column run side by side; the
+// nine-to-three combine and the RK4 recursion go through shared memory. The
+// last CTA takes the packed kx = 0 / N/2 columns.
+template <typename real, int N, int W, int E>
+__global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __grid_constant__ AdjArgs<real> a) {
+    constexpr int H = N / 2, TEAM = N / E, NXH = H + 1;
+    constexpr int SPAN = N * (W > 1 ? W : 2);   // complex per team buffer (the edge CTA needs 2N)
+    constexpr int NTH = NGA * W * TEAM;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    cplx<real>* xb = reinterpret_cast<cplx<real>*>(smem_raw);
-    const int r = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
-    const int n = blockIdx.x * ROWS + r;
-    XchgRow<real> x{xb + r * H};
-    real* gs = reinterpret_cast<real*>(xb + ROWS * H) + (size_t)r * NGA * N;
-    TeamFFT<real, H, E> fft;
+    cplx<real>* sm = reinterpret_cast<cplx<real>*>(smem_raw);
+    const int tid = threadIdx.x;
+    const int f = tid / (W * TEAM), rem = tid % (W * TEAM);
+    const int w = rem % W, t = rem / W;
+    cplx<real>* buf = sm + (size_t)f * SPAN;
+    XchgCols<real> x{buf, w, W};
+    TeamFFT<real, N, E> fft;
     fft.template init<N>(t, a.tw);
+    const bool edge = blockIdx.x == gridDim.x - 1;
+    const bool emit_q = f < NGA && (a.advect || f > GA_VW);
+    const real n2 = (real)1 / ((real)N * (real)N);
 
-    // 1. g_q rows by C2R (slot 0 of each T row holds DC + i Nyquist)
-#pragma unroll 1
-    for (int q = 0; q < NGA; ++q) {
-        if (!a.advect && q <= GA_VW) {
+    if (!edge) {
+        const int i = blockIdx.x * W + w;
+        const bool active = i != 0;
+        const real kx = a.dkx * (real)i;
+        if (a.stage >= 1) {
+            const bool mine = f < PF_COUNT && active;
+            cplx<real> v[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+                v[e] = mine ? a.Tx[(size_t)f * N * H + (size_t)(t + TEAM * e) * H + i] : mk<real>(0, 0);
+            fft.template run<false>(t, v, x);
+            if (f < PF_COUNT)
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int j = t + TEAM * e;
+                    const real ky = ky_of<real>(j, N, a.dky);
+                    const real k2 = kx * kx + ky * ky;
+                    buf[j * W + w] = adj_cmult<real>(f, v[e], kx, ky, k2 > 0 ? (real)1 / k2 : (real)0);
+                }
+        }
+        __syncthreads();
+        for (int pt = tid; pt < N * W; pt += NTH) {
+            const int j = pt / W, w2 = pt % W, i2 = blockIdx.x * W + w2;
+            if (i2 == 0) continue;
+            cplx<real> cb[3] = {mk<real>(0, 0), mk<real>(0, 0), mk<real>(0, 0)};
+            if (a.stage >= 1)
+#pragma unroll
+                for (int p = 0; p < PF_COUNT; ++p) cb[adj_target(p)] = cadd(cb[adj_target(p)], sm[(size_t)p * SPAN + j * W + w2]);
+            const size_t idx = (size_t)j * NXH + i2;
+            const bool keep = adj_keep(a, i2, j);
+            const cplx<real> lossg = a.wstate ? cscale(a.wstate[idx], 2 * a.loss_w * n2 * n2) : mk<real>(0, 0);
+#pragma unroll
+            for (int g = 0; g < 3; ++g) {
+                real Ef, Eh;
+                adj_factors<real, N>(a, g, i2, j, Ef, Eh);
+                sm[(size_t)g * SPAN + j * W + w2] =
+                    adj_rk(a, g, idx, cscale(cb[g], 2 * n2), Ef, Eh, keep, g == 0 ? lossg : mk<real>(0, 0));
+            }
+        }
+        __syncthreads();
+        if (!a.emit) return;
+        cplx<real> v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int j = t + TEAM * e;
+            v[e] = mk<real>(0, 0);
+            if (emit_q && active) {
+                const cplx<real> lw = sm[j * W + w], l1 = sm[SPAN + j * W + w], l2 = sm[2 * SPAN + j * W + w];
+                v[e] = cscale(adj_emit<real>(f, lw, l1, l2, kx, ky_of<real>(j, N, a.dky), a.ce), (real)0.5);
+            }
+        }
+        __syncthreads();
+        fft.template run<true>(t, v, x);
+        if (emit_q && active)
+#pragma unroll
+            for (int e = 0; e < E; ++e) a.Tg[(size_t)f * N * H + (size_t)(t + TEAM * e) * H + i] = v[e];
+        return;
+    }
+
+    // ---- the kx = 0 and kx = N/2 columns, packed as DC + i Nyquist; lanes w == 0 of each team
+    const bool lead = w == 0;
+    const real kN = a.dkx * (real)H;
+    {
+        const bool mine = f < PF_COUNT && lead && a.stage >= 1;
+        cplx<real> v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = mine ? a.Tx[(size_t)f * N * H + (size_t)(t + TEAM * e) * H] : mk<real>(0, 0);
+        fft.template run<false>(t, v, x);
+        if (lead)
+#pragma unroll
+            for (int e = 0; e < E; ++e) buf[(t + TEAM * e) * W] = v[e];
+        __syncthreads();
+        cplx<real> zm[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) zm[e] = lead ? cconj(buf[((N - (t + TEAM * e)) % N) * W]) : mk<real>(0, 0);
+        __syncthreads();
+        if (f < PF_COUNT && lead)
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                const int m = t + TEAM * e;
-                gs[q * N + 2 * m] = 0;
-                gs[q * N + 2 * m + 1] = 0;
+                const int j = t + TEAM * e;
+                const real ky = ky_of<real>(j, N, a.dky);
+                const cplx<real> z0 = a.stage >= 1 ? cscale(cadd(v[e], zm[e]), (real)0.5) : mk<real>(0, 0);
+                const cplx<real> zH = a.stage >= 1 ? cmul_mi(cscale(csub(v[e], zm[e]), (real)0.5)) : mk<real>(0, 0);
+                const real k2H = kN * kN + ky * ky;
+                buf[j] = adj_cmult<real>(f, z0, (real)0, ky, ky != 0 ? (real)1 / (ky * ky) : (real)0);
+                buf[N + j] = adj_cmult<real>(f, zH, kN, ky, k2H > 0 ? (real)1 / k2H : (real)0);
             }
-            continue;
+    }
+    __syncthreads();
+    for (int pt = tid; pt < 2 * N; pt += NTH) {
+        const int c = pt / N, j = pt % N, jm = (N - j) % N;
+        const int i = c == 0 ? 0 : H;
+        cplx<real> cb[3] = {mk<real>(0, 0), mk<real>(0, 0), mk<real>(0, 0)};
+#pragma unroll
+        for (int p = 0; p < PF_COUNT; ++p) cb[adj_target(p)] = cadd(cb[adj_target(p)], sm[(size_t)p * SPAN + c * N + j]);
+        const size_t idx = (size_t)j * NXH + i;
+        cplx<real> lossg = mk<real>(0, 0);
+        if (a.wstate) {
+            const cplx<real> P = cscale(cadd(a.wstate[idx], cconj(a.wstate[(size_t)jm * NXH + i])), (real)0.5);
+            lossg = cscale(P, a.loss_w * n2 * n2);
         }
-        const cplx<real>* row = a.Tg + (size_t)q * N * H + (size_t)n * H;
+        const bool keep = adj_keep(a, i, j);
+#pragma unroll
+        for (int g = 0; g < 3; ++g) {
+            real Ef, Eh;
+            adj_factors<real, N>(a, g, i, j, Ef, Eh);
+            sm[(size_t)g * SPAN + c * N + j] =
+                adj_rk(a, g, idx, cscale(cb[g], n2), Ef, Eh, keep, g == 0 ? lossg : mk<real>(0, 0));
+        }
+    }
+    __syncthreads();
+    if (!a.emit) return;
+    cplx<real> v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        v[e] = mk<real>(0, 0);
+        if (!(emit_q && lead)) continue;
+        const int j = t + TEAM * e;
+        cplx<real> P[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const real kx = c == 0 ? (real)0 : kN;
+            cplx<real> val[2];
+#pragma unroll
+            for (int s2 = 0; s2 < 2; ++s2) {
+                const int jj = s2 == 0 ? j : (N - j) % N, jp = (N - jj) % N;
+                cplx<real> lw = sm[c * N + jj];
+                if (f <= GA_VW) lw = cscale(cadd(lw, cconj(sm[c * N + jp])), (real)0.5);
+                const cplx<real> l1 = sm[SPAN + c * N + jj], l2 = sm[2 * SPAN + c * N + jj];
+                val[s2] = adj_emit<real>(f, lw, l1, l2, kx, ky_of<real>(jj, N, a.dky), a.ce);
+            }
+            P[c] = cscale(cadd(val[0], cconj(val[1])), (real)0.5);
+        }
+        v[e] = cadd(P[0], cmul_i(P[1]));
+    }
+    __syncthreads();
+    fft.template run<true>(t, v, x);
+    if (emit_q && lead)
+#pragma unroll
+        for (int e = 0; e < E; ++e) a.Tg[(size_t)f * N * H + (size_t)(t + TEAM * e) * H] = v[e];
+}
+
+// Field-parallel row kernel: one team of H/E threads per (transform, row),
+// NGA teams per row (half-length real transforms): the 11 C2R of the g rows
+// side by side, the transposed products at each point of the row against the
+// nine recorded forward fields (activity gradient accumulated in place), then
+// the 9 R2C side by side. A team's exchange buffer (H complex = N reals) holds
+// its real row between the transforms.
+template <typename real, int N, int E>
+__global__ void __launch_bounds__(NGA * (N / 2 / E)) adj_row_kernel(const __grid_constant__ AdjArgs<real> a) {
+    constexpr int H = N / 2, TEAM = H / E, TPR = NGA * TEAM;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cplx<real>* sm = reinterpret_cast<cplx<real>*>(smem_raw);
+    const int q = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
+    const int n = blockIdx.x;
+    cplx<real>* buf = sm + (size_t)q * H;
+    real* row = reinterpret_cast<real*>(buf);
+    const real* rows = reinterpret_cast<const real*>(sm);   // field q at rows[q * N + x]
+    XchgRow<real> x{buf};
+    TeamFFT<real, H, E> fft;
+    fft.template init<N>(t, a.tw);
+    const bool live = a.advect || q > GA_VW;
+
+    // 1. g_q = C2R of row n of Tg[q] (slot 0 of a T row holds DC + i Nyquist)
+    {
+        const cplx<real>* tr = a.Tg + (size_t)q * N * H + (size_t)n * H;
         cplx<real> v[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int k = t + TEAM * e;
+            v[e] = mk<real>(0, 0);
+            if (!live) continue;
             if (k == 0) {
-                const cplx<real> d = row[0];
+                const cplx<real> d = tr[0];
                 v[e] = mk<real>(d.x + d.y, d.x - d.y);
             } else {
-                const cplx<real> A = row[k], B = cconj(row[H - k]);
+                const cplx<real> A = tr[k], B = cconj(tr[H - k]);
                 v[e] = cadd(cadd(A, B), cmul_i(cmul(cconj(a.tw[k]), csub(A, B))));
             }
         }
@@ -369,73 +551,61 @@ __global__ void __launch_bounds__(ROWS * (N / 2 / E)) adj_row_kernel(const __gri
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int m = t + TEAM * e;
-            gs[q * N + 2 * m] = v[e].x;
-            gs[q * N + 2 * m + 1] = v[e].y;
+            row[2 * m] = v[e].x;
+            row[2 * m + 1] = v[e].y;
         }
     }
+    __syncthreads();
 
-    // 2. transposed products; the adjoints overwrite slots 0..8 of this point
+    // 2. transposed products at each point of the row
     const real lam = a.lambda;
-    const size_t rb = (size_t)n * N;
     const size_t NN = (size_t)N * N;
-#pragma unroll 1
-    for (int e = 0; e < E; ++e) {
+    real* rw = reinterpret_cast<real*>(sm);
+    for (int xi = threadIdx.x; xi < N; xi += TPR) {
+        const size_t pi = (size_t)n * N + xi;
+        const real w = a.phys[PF_W * NN + pi], r1 = a.phys[PF_R1 * NN + pi], r2 = a.phys[PF_R2 * NN + pi];
+        const real u = a.phys[PF_U * NN + pi], v = a.phys[PF_V * NN + pi], ux = a.phys[PF_UX * NN + pi];
+        const real sh = a.phys[PF_SH * NN + pi], L1 = a.phys[PF_LR1 * NN + pi], L2 = a.phys[PF_LR2 * NN + pi];
+        const real al = a.alpha_field ? a.alpha_field[pi] : a.alpha;
+        real g[NGA];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int xi = 2 * (t + TEAM * e) + h;
-            const size_t pi = rb + xi;
-            const real w = a.phys[PF_W * NN + pi], r1 = a.phys[PF_R1 * NN + pi], r2 = a.phys[PF_R2 * NN + pi];
-            const real u = a.phys[PF_U * NN + pi], v = a.phys[PF_V * NN + pi], ux = a.phys[PF_UX * NN + pi];
-            const real sh = a.phys[PF_SH * NN + pi], L1 = a.phys[PF_LR1 * NN + pi], L2 = a.phys[PF_LR2 * NN + pi];
-            const real al = a.alpha_field ? a.alpha_field[pi] : a.alpha;
-            real g[NGA];
-#pragma unroll
-            for (int q = 0; q < NGA; ++q) g[q] = gs[q * N + xi];
-            const real S = 2 * sqrt(r1 * r1 + r2 * r2);
-            const real sgl = lam * S * (S * S - 1);
-            const real dsgl = lam * (3 * S * S - 1);
-            const real g1221 = g[GA_P12] + g[GA_P21];
-            const real Sb = (-lam * L1 + dsgl * r1) * g[GA_P11] + (-lam * L2 + dsgl * r2) * g1221 +
-                            (-2 * S * r1 + lam * ux) * g[GA_A1] + (-2 * S * r2 + (real)0.5 * lam * sh) * g[GA_A2];
-            const real dS1 = S > 0 ? 4 * r1 / S : (real)0, dS2 = S > 0 ? 4 * r2 / S : (real)0;
-            const real wb = -u * g[GA_UW] - v * g[GA_VW] - r2 * g[GA_A1] + r1 * g[GA_A2];
-            const real r1b = (sgl - al) * g[GA_P11] - 2 * L2 * g[GA_P12] + 2 * L2 * g[GA_P21] - S * S * g[GA_A1] -
+        for (int k = 0; k < NGA; ++k) g[k] = rows[k * N + xi];
+        const real S = 2 * sqrt(r1 * r1 + r2 * r2);
+        const real sgl = lam * S * (S * S - 1);
+        const real dsgl = lam * (3 * S * S - 1);
+        const real g1221 = g[GA_P12] + g[GA_P21];
+        const real Sb = (-lam * L1 + dsgl * r1) * g[GA_P11] + (-lam * L2 + dsgl * r2) * g1221 +
+                        (-2 * S * r1 + lam * ux) * g[GA_A1] + (-2 * S * r2 + (real)0.5 * lam * sh) * g[GA_A2];
+        const real dS1 = S > 0 ? 4 * r1 / S : (real)0, dS2 = S > 0 ? 4 * r2 / S : (real)0;
+        if (a.alpha_grad) a.alpha_grad[pi] += -(r1 * g[GA_P11] + r2 * g1221);
+        rw[PF_W * N + xi] = -u * g[GA_UW] - v * g[GA_VW] - r2 * g[GA_A1] + r1 * g[GA_A2];
+        rw[PF_R1 * N + xi] = (sgl - al) * g[GA_P11] - 2 * L2 * g[GA_P12] + 2 * L2 * g[GA_P21] - S * S * g[GA_A1] -
                              u * g[GA_UR1] - v * g[GA_VR1] + w * g[GA_A2] + Sb * dS1;
-            const real r2b = (sgl + 2 * L1 - al) * g[GA_P12] + (sgl - 2 * L1 - al) * g[GA_P21] - w * g[GA_A1] -
+        rw[PF_R2 * N + xi] = (sgl + 2 * L1 - al) * g[GA_P12] + (sgl - 2 * L1 - al) * g[GA_P21] - w * g[GA_A1] -
                              S * S * g[GA_A2] - u * g[GA_UR2] - v * g[GA_VR2] + Sb * dS2;
-            const real ub = -w * g[GA_UW] - r1 * g[GA_UR1] - r2 * g[GA_UR2];
-            const real vb = -w * g[GA_VW] - r1 * g[GA_VR1] - r2 * g[GA_VR2];
-            const real uxb = lam * S * g[GA_A1];
-            const real shb = (real)0.5 * lam * S * g[GA_A2];
-            const real L1b = -lam * S * g[GA_P11] + 2 * r2 * g[GA_P12] - 2 * r2 * g[GA_P21];
-            const real L2b = (-lam * S - 2 * r1) * g[GA_P12] + (-lam * S + 2 * r1) * g[GA_P21];
-            if (a.alpha_grad) a.alpha_grad[pi] += -(r1 * g[GA_P11] + r2 * g1221);
-            gs[PF_W * N + xi] = wb;
-            gs[PF_R1 * N + xi] = r1b;
-            gs[PF_R2 * N + xi] = r2b;
-            gs[PF_U * N + xi] = ub;
-            gs[PF_V * N + xi] = vb;
-            gs[PF_UX * N + xi] = uxb;
-            gs[PF_SH * N + xi] = shb;
-            gs[PF_LR1 * N + xi] = L1b;
-            gs[PF_LR2 * N + xi] = L2b;
-        }
+        rw[PF_U * N + xi] = -w * g[GA_UW] - r1 * g[GA_UR1] - r2 * g[GA_UR2];
+        rw[PF_V * N + xi] = -w * g[GA_VW] - r1 * g[GA_VR1] - r2 * g[GA_VR2];
+        rw[PF_UX * N + xi] = lam * S * g[GA_A1];
+        rw[PF_SH * N + xi] = (real)0.5 * lam * S * g[GA_A2];
+        rw[PF_LR1 * N + xi] = -lam * S * g[GA_P11] + 2 * r2 * g[GA_P12] - 2 * r2 * g[GA_P21];
+        rw[PF_LR2 * N + xi] = (-lam * S - 2 * r1) * g[GA_P12] + (-lam * S + 2 * r1) * g[GA_P21];
     }
+    __syncthreads();
 
-    // 3. R2C of the 9 adjoints into Tx (slot 0: DC + i Nyquist)
-#pragma unroll 1
-    for (int p = 0; p < PF_COUNT; ++p) {
-        cplx<real> v[E];
+    // 3. R2C of the nine adjoints (teams 0..8) into Tx
+    cplx<real> v[E];
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int m = t + TEAM * e;
-            v[e] = mk<real>(gs[p * N + 2 * m], gs[p * N + 2 * m + 1]);
-        }
-        fft.template run<false>(t, v, x);
+    for (int e = 0; e < E; ++e) {
+        const int m = t + TEAM * e;
+        v[e] = q < PF_COUNT ? mk<real>(row[2 * m], row[2 * m + 1]) : mk<real>(0, 0);
+    }
+    __syncthreads();
+    fft.template run<false>(t, v, x);
 #pragma unroll
-        for (int e = 0; e < E; ++e) x.write(t + TEAM * e, v[e]);
-        x.sync();
-        cplx<real>* out = a.Tx + (size_t)p * N * H + (size_t)n * H;
+    for (int e = 0; e < E; ++e) x.write(t + TEAM * e, v[e]);
+    x.sync();
+    if (q < PF_COUNT) {
+        cplx<real>* out = a.Tx + (size_t)q * N * H + (size_t)n * H;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int k = t + TEAM * e;
@@ -448,7 +618,6 @@ __global__ void __launch_bounds__(ROWS * (N / 2 / E)) adj_row_kernel(const __gri
                 out[k] = csub(sum, cmul_i(cmul(a.tw[k], dif)));
             }
         }
-        x.sync();
     }
 }
 

@@ -1643,14 +1643,25 @@ struct OpAdjBackward {
                           cudaStream_t st) {
         using C = Cfg<real, N>;
         constexpr int H = N / 2;
-        constexpr int W = C::W, EC = C::EC, ER = C::ERT, ROWS = C::ROWS_T;
-        constexpr int COL_THREADS = W * (N / EC), ROW_THREADS = ROWS * (H / ER);
-        constexpr size_t COL_SMEM = (size_t)W * N * sizeof(cplx<real>);
-        constexpr size_t ROW_SMEM = (size_t)ROWS * (H * sizeof(cplx<real>) + (size_t)NGA * N * sizeof(real));
+        // column pass: field-parallel (11 transform teams per column, one column per CTA) up to 256^2,
+        // W columns per CTA with the transforms in sequence above
+        constexpr bool FP = N <= 256;
+        constexpr int W = FP ? 1 : C::W;
+        constexpr int EC = FP ? (N / 16 > 4 ? N / 16 : 4) : C::EC;
+        constexpr int COL_THREADS = FP ? NGA * W * (N / EC) : W * (N / EC);
+        constexpr size_t COL_SMEM = FP ? (size_t)NGA * N * (W > 1 ? W : 2) * sizeof(cplx<real>)
+                                       : (size_t)W * N * sizeof(cplx<real>);
+        // row pass: field-parallel, teams of H/ER threads (16 from 128^2 up)
+        constexpr int ER = H / 16 < 2 ? 2 : (H / 16 > 16 ? 16 : H / 16);
+        constexpr int ROW_THREADS = NGA * (H / ER);
+        constexpr size_t ROW_SMEM = (size_t)NGA * H * sizeof(cplx<real>);
         static bool attrs = false;
         if (!attrs) {
-            QAF_CUDA(cudaFuncSetAttribute(adj_col_kernel<real, N, W, EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COL_SMEM));
-            QAF_CUDA(cudaFuncSetAttribute(adj_row_kernel<real, N, ER, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROW_SMEM));
+            if constexpr (FP)
+                QAF_CUDA(cudaFuncSetAttribute(adj_colp_kernel<real, N, W, EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COL_SMEM));
+            else
+                QAF_CUDA(cudaFuncSetAttribute(adj_col_kernel<real, N, W, EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COL_SMEM));
+            QAF_CUDA(cudaFuncSetAttribute(adj_row_kernel<real, N, ER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROW_SMEM));
             attrs = true;
         }
         qaf_mesh* m = A->m;
@@ -1689,7 +1700,8 @@ struct OpAdjBackward {
         const int T = A->nsteps;
         auto in_window = [&](int n) { return A->window > 0 && gloss != 0.0 && n >= T - A->window + 1; };
         auto col = [&]() {
-            adj_col_kernel<real, N, W, EC><<<H / W + 1, COL_THREADS, COL_SMEM, st>>>(a);
+            if constexpr (FP) adj_colp_kernel<real, N, W, EC><<<H / W + 1, COL_THREADS, COL_SMEM, st>>>(a);
+            else adj_col_kernel<real, N, W, EC><<<H / W + 1, COL_THREADS, COL_SMEM, st>>>(a);
             m->launches += 1;
         };
         bool started = false;
@@ -1713,7 +1725,7 @@ struct OpAdjBackward {
                 }
                 for (int s = 4; s >= 1; --s) {
                     a.phys = reinterpret_cast<const real*>(A->phys) + ((size_t)(n - t0) * 4 + (s - 1)) * slot;
-                    adj_row_kernel<real, N, ER, ROWS><<<N / ROWS, ROW_THREADS, ROW_SMEM, st>>>(a);
+                    adj_row_kernel<real, N, ER><<<N, ROW_THREADS, ROW_SMEM, st>>>(a);
                     m->launches += 1;
                     a.stage = s;
                     a.emit = (s > 1 || n > 0) ? 1 : 0;

@@ -80,6 +80,20 @@ def test_gradient_matches_oracle_tlm_fp64(cuda, advect):
         assert abs(got - want) <= 1e-9 * abs(want), (trial, got, want)
 
 
+@pytest.mark.parametrize("n", [16, 64, 128, 256, 512])
+def test_gradient_matches_oracle_tlm_all_sizes(cuda, n):
+    """Every launch shape of the adjoint kernels (field-parallel up to 256^2, column-sequential above)."""
+    import qaf
+    T, K, Wn, dt = 3, 2, 2, 5e-3
+    p, s0, alpha, gT, rng = _setup(n, 21, dt)
+    _, _, g, ga = _gpu_grad(qaf, n, qaf.F64, s0, alpha, gT, T, K, Wn, dt)
+    d = [rng.standard_normal(s0[0].shape) + 1j * rng.standard_normal(s0[0].shape) for _ in range(3)]
+    dal = rng.standard_normal((n, n))
+    want = _tlm_dJ(p, s0, alpha, d, dal, gT, T, Wn)
+    got = _dot(g, d) + float(np.sum(ga * dal))
+    assert abs(got - want) <= 1e-9 * abs(want), (got, want)
+
+
 def test_gradient_separate_directions_fp64(cuda):
     """State-only and activity-only directions, loss-only and final-state-only objectives."""
     import qaf
