@@ -81,6 +81,7 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
     ap.add_argument("--workload", choices=["plain", "ensemble", "adjoint"], default="plain")
     ap.add_argument("--no-fd", action="store_true", help="adjoint workload: skip the finite-difference check")
+    ap.add_argument("--no-tune", action="store_true", help="ensemble workload: keep the built-in launch shapes")
     ap.add_argument("--instances", type=int, default=ENS_COUNT)
     return ap.parse_args()
 
@@ -380,7 +381,9 @@ def run_ensemble(a, world, rank, local):
     rf = [rf_all[k] for k in mine]
     seeds = [seed_all[k] for k in mine]
     p = qaf.Params(re=1.0, er=1.0, rf=0.0, lam=0.1, alpha=1.0, dt=ENS_DT, q_lin=1.0, advect_omega=1)
-    ens = qaf.Ensemble(sizes, p, alpha, rf, lx=L, dtype=qaf.F32)
+    import tempfile
+    tune_cache = os.path.join(tempfile.mkdtemp(prefix="qaf_tune_"), "autotune.jsonl")
+    ens = qaf.Ensemble(sizes, p, alpha, rf, lx=L, dtype=qaf.F32, tune=not a.no_tune, tune_cache=tune_cache)
     ens.init_random(seeds)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     work_mine = sum(n * n for n in sizes)
@@ -459,6 +462,7 @@ def run_ensemble(a, world, rank, local):
         "data": "synthetic (seeded instance table; seeded random Q ~ U(-0.01,0.01), w = 0 per instance)",
         "config": {"workload": ens_workload_desc(a.instances), "instances": a.instances,
                    "sizes": {str(n): n_all.count(n) for n in sorted(set(n_all))},
+                   "launch_shapes": ens.tuned,
                    "parallelism": f"instances sharded over {world} rank(s)",
                    "l2": "flushed (256 MiB write) between timed steps"},
         "looped": {"value": looped, "unit": UNIT, "steps": loop_steps, "ms_per_step": ms_loop / loop_steps,

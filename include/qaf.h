@@ -198,6 +198,28 @@ qaf_status qaf_ensemble_set_controls(qaf_ensemble* ens, const double* alpha, con
 /* synchronises `stream`; out[2k], out[2k+1] = energy, enstrophy of instance k after the last step */
 qaf_status qaf_ensemble_diagnostics(qaf_ensemble* ens, double* out, void* stream);
 
+/* ---- launch-shape autotuner --------------------------------------------------
+ * No counterpart in the reference. The fused step kernels have alternative
+ * launch shapes (FP32, grids 64, 128, 256, 1024: FFT radix per thread, rows per
+ * CTA); a library-wide table picks one column and one row shape per (precision,
+ * n, batched = more than one instance per launch), used by every launch made
+ * after the choice (ensembles: those created after it). Default: the built-in
+ * shapes.
+ * qaf_autotune: times each shape on `ninst` synthetic instances of n x n, keeps
+ *   the fastest, and (cache_path != NULL) records it in a JSON-lines file, one
+ *   record per (device, precision, n, batched). choice: "col:<name> row:<name>".
+ * qaf_autotune_load: applies the records of a cache file that match this GPU
+ *   (or whose device is "*"); records naming unknown shapes are skipped.
+ * qaf_set_variant / qaf_variant_choice / qaf_variant_list: set, read and list
+ *   the shapes by name ("default" or a listed name). */
+qaf_status qaf_autotune(int n, qaf_dtype dtype, int ninst, const char* cache_path, char* choice, int choice_len,
+                        double* us_per_step);
+qaf_status qaf_autotune_load(const char* cache_path);
+qaf_status qaf_autotune_reset(void);
+qaf_status qaf_set_variant(int n, qaf_dtype dtype, int batched, const char* col, const char* row);
+qaf_status qaf_variant_choice(int n, qaf_dtype dtype, int batched, char* buf, int len);
+qaf_status qaf_variant_list(int n, qaf_dtype dtype, char* buf, int len);
+
 /* ---- discrete adjoint (IF-RK4) ---------------------------------------------
  * No counterpart in the reference (it has no gradients): reverse-mode
  * derivatives of `nsteps` IF-RK4 steps (qaf_state_advance) with respect to the

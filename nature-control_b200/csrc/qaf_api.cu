@@ -7,12 +7,17 @@
 #include "qaf_kernels.cuh"
 #include "qaf_ops.cuh"
 #include "qaf_adjoint.cuh"
+#include "qaf_variants.cuh"
 
 #include <cmath>
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <fstream>
+#include <map>
 #include <mutex>
+#include <sstream>
+#include <tuple>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -289,6 +294,48 @@ StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
 }
 
 // ---------------------------------------------------------------------------
+// launch-shape choices (autotuner): per (precision, grid size, batched) the
+// column and row variants to use instead of the built-in shapes; -1 = built in
+// ---------------------------------------------------------------------------
+struct TuneChoice {
+    int col = -1, row = -1;
+    double us = 0;
+};
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, TuneChoice> g_tune;
+
+int variant_list(int dtype, int n, StepVariant<float>** out) {
+    *out = nullptr;
+    return dtype == QAF_F32 ? step_variants_f32(n, out) : 0;
+}
+
+// the variant to launch for kind (0 column, 1 row), or nullptr for the built-in shape
+StepVariant<float>* tuned_variant(int n, int kind, bool batched) {
+    int idx = -1;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        if (g_tune.empty()) return nullptr;
+        auto it = g_tune.find(std::make_tuple((int)QAF_F32, n, batched ? 1 : 0));
+        if (it == g_tune.end()) return nullptr;
+        idx = kind == 0 ? it->second.col : it->second.row;
+    }
+    if (idx < 0) return nullptr;
+    StepVariant<float>* v = nullptr;
+    const int cnt = step_variants_f32(n, &v);
+    if (idx >= cnt) return nullptr;
+    if (v[idx].slots == 0 && v[idx].kind == 0) {
+        int slots = 0;
+        if (v[idx].setup(&slots) != cudaSuccess || slots < 1) return nullptr;
+        v[idx].slots = slots;
+    } else if (v[idx].kind == 1 && v[idx].slots == 0) {
+        int unused = 0;
+        if (v[idx].setup(&unused) != cudaSuccess) return nullptr;
+        v[idx].slots = -1;   // set up
+    }
+    return &v[idx];
+}
+
+// ---------------------------------------------------------------------------
 // per-size launchers
 // ---------------------------------------------------------------------------
 template <typename real, int N>
@@ -313,11 +360,23 @@ struct Launch {
         return QAF_OK;
     }
     static void col(const StageArgs<real>& a, cudaStream_t st) {
+        if constexpr (std::is_same<real, float>::value) {
+            if (StepVariant<float>* v = tuned_variant(N, 0, a.ninst > 1)) {
+                v->launch(a, v->slots, st);
+                return;
+            }
+        }
         const long items = (long)C::COL_ITEMS * a.ninst;
         const int grid = items < col_slots ? (int)items : col_slots;
         col_kernel<real, N, C::EC, C::MINB><<<grid, C::COL_THREADS, C::COL_SMEM, st>>>(a);
     }
     static void row(const StageArgs<real>& a, cudaStream_t st) {
+        if constexpr (std::is_same<real, float>::value) {
+            if (StepVariant<float>* v = tuned_variant(N, 1, a.ninst > 1)) {
+                v->launch(a, v->slots, st);
+                return;
+            }
+        }
         row_kernel<real, N, C::ER, C::ROWS, C::MINB><<<C::ROW_BLOCKS * a.ninst, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
     }
     static void bwd(const cplx<real>* spec, cplx<real>* T, real* phys, const cplx<real>* tw, cudaStream_t st) {
@@ -1820,6 +1879,269 @@ qaf_status qaf_adjoint_backward(qaf_adjoint* A, const void* gwT, const void* gr1
     void* g0[3] = {gw0, gr1_0, gr2_0};
     return dispatch<OpAdjBackward>(A->m, A, (const void* const*)gT, gloss, (void* const*)g0, galpha,
                                    (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Autotuner: times the launch variants of the fused step kernels on a
+// synthetic ensemble and keeps the fastest per (precision, grid size,
+// batched); the choices persist in a JSON-lines cache.
+// ===========================================================================
+namespace {
+
+// one IF-RK4 step of every group of the ensemble, launched directly (not the captured graph)
+template <typename real>
+qaf_status ens_step_direct(qaf_ensemble* e, cudaStream_t st) {
+    for (auto& g : groups<real>(e)) {
+        StageArgs<real> a = group_args<real>(e, g);
+        a.mode = MODE_STAGE;
+        a.do_inverse = 1;
+        a.diag = nullptr;
+        qaf_status s2 = with_n(g.N, [&](auto n) -> qaf_status {
+            for (int k = 1; k <= 4; ++k) {
+                a.stage = k;
+                a.last_stage = k == 4;
+                Launch<real, decltype(n)::value>::row(a, st);
+                Launch<real, decltype(n)::value>::col(a, st);
+            }
+            return QAF_OK;
+        });
+        if (s2 != QAF_OK) return s2;
+    }
+    return post_launch("autotune step");
+}
+
+std::string device_name() {
+    int dev = 0;
+    cudaDeviceProp prop;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return "";
+    }
+    return prop.name;
+}
+
+std::string variant_name(int dtype, int n, int kind, int idx) {
+    if (idx < 0) return kind == 0 ? "col:default" : "row:default";
+    StepVariant<float>* v = nullptr;
+    const int cnt = variant_list(dtype, n, &v);
+    return idx < cnt ? v[idx].name : "?";
+}
+
+// index of a variant by name: -1 for "<kind>:default" or "default", -2 if unknown
+int variant_index(int dtype, int n, int kind, const std::string& name) {
+    if (name == "default" || name == (kind == 0 ? "col:default" : "row:default")) return -1;
+    StepVariant<float>* v = nullptr;
+    const int cnt = variant_list(dtype, n, &v);
+    for (int i = 0; i < cnt; ++i)
+        if (v[i].kind == kind && name == v[i].name) return i;
+    return -2;
+}
+
+void set_choice(int dtype, int n, int batched, int col, int row, double us) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    TuneChoice c;
+    c.col = col; c.row = row; c.us = us;
+    g_tune[std::make_tuple(dtype, n, batched)] = c;
+}
+
+// the value of "key": in one JSON-lines record (string or number, as text)
+bool json_field(const std::string& line, const std::string& key, std::string& out) {
+    const std::string pat = "\"" + key + "\":";
+    size_t p = line.find(pat);
+    if (p == std::string::npos) return false;
+    p += pat.size();
+    while (p < line.size() && line[p] == ' ') ++p;
+    if (p < line.size() && line[p] == '"') {
+        const size_t q = line.find('"', p + 1);
+        if (q == std::string::npos) return false;
+        out = line.substr(p + 1, q - p - 1);
+        return true;
+    }
+    size_t q = p;
+    while (q < line.size() && line[q] != ',' && line[q] != '}') ++q;
+    out = line.substr(p, q - p);
+    return !out.empty();
+}
+
+std::string cache_record(const std::string& dev, int dtype, int n, int batched, int col, int row, double us) {
+    std::ostringstream o;
+    o << "{\"device\": \"" << dev << "\", \"dtype\": \"" << (dtype == QAF_F64 ? "f64" : "f32") << "\", \"n\": " << n
+      << ", \"batched\": " << batched << ", \"col\": \"" << variant_name(dtype, n, 0, col) << "\", \"row\": \""
+      << variant_name(dtype, n, 1, row) << "\", \"us_per_step\": " << us << "}";
+    return o.str();
+}
+
+qaf_status cache_write(const char* path, const std::string& dev, int dtype, int n, int batched, const std::string& rec) {
+    std::vector<std::string> keep;
+    {
+        std::ifstream in(path);
+        std::string line;
+        while (std::getline(in, line)) {
+            std::string d, t, nn, b;
+            if (json_field(line, "device", d) && json_field(line, "dtype", t) && json_field(line, "n", nn) &&
+                json_field(line, "batched", b) && d == dev && t == (dtype == QAF_F64 ? "f64" : "f32") &&
+                std::atoi(nn.c_str()) == n && std::atoi(b.c_str()) == batched)
+                continue;   // replaced below
+            if (!line.empty()) keep.push_back(line);
+        }
+    }
+    keep.push_back(rec);
+    const std::string tmp = std::string(path) + ".tmp";
+    {
+        std::ofstream out(tmp, std::ios::trunc);
+        if (!out) return fail(QAF_ERR_INVALID, std::string("cannot write ") + tmp);
+        for (auto& l : keep) out << l << "\n";
+    }
+    if (std::rename(tmp.c_str(), path) != 0) return fail(QAF_ERR_INVALID, std::string("cannot replace ") + path);
+    return QAF_OK;
+}
+
+template <typename real>
+qaf_status autotune_impl(int n, int ninst, int dtype, double* best_us, int* best_col, int* best_row) {
+    std::vector<int> sizes(ninst, n);
+    std::vector<double> alpha(ninst, 1.0), rf(ninst, 0.1);
+    std::vector<uint64_t> seeds(ninst);
+    for (int k = 0; k < ninst; ++k) seeds[k] = 1000 + k;
+    qaf_params p{};
+    p.re = 1; p.er = 1; p.rf = 0.1; p.lambda = 0.1; p.alpha = 1; p.alpha_field = nullptr; p.dt = 1e-3; p.q_lin = 1;
+    p.advect_omega = 1;
+    qaf_ensemble* e = nullptr;
+    QAF_TRY(qaf_ensemble_create(ninst, sizes.data(), 16 * M_PI, 16 * M_PI, (qaf_dtype)dtype, &p, alpha.data(),
+                                rf.data(), &e));
+    struct Guard { qaf_ensemble* e; ~Guard() { qaf_ensemble_destroy(e); } } guard{e};
+    cudaStream_t st = nullptr;
+    QAF_TRY(qaf_ensemble_init_random(e, seeds.data(), -0.01, 0.01, st));
+    QAF_TRY(qaf_ensemble_advance(e, 0, st));   // prologue
+    const int batched = ninst > 1 ? 1 : 0;
+    cudaEvent_t e0, e1;
+    QAF_CUDA(cudaEventCreate(&e0));
+    QAF_CUDA(cudaEventCreate(&e1));
+    auto time_choice = [&](int col, int row, double* us) -> qaf_status {
+        set_choice(dtype, n, batched, col, row, 0);
+        for (int w = 0; w < 3; ++w) QAF_TRY(ens_step_direct<real>(e, st));
+        const int reps = 20;
+        QAF_CUDA(cudaEventRecord(e0, st));
+        for (int r = 0; r < reps; ++r) QAF_TRY(ens_step_direct<real>(e, st));
+        QAF_CUDA(cudaEventRecord(e1, st));
+        QAF_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        QAF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        *us = 1e3 * ms / reps;
+        return QAF_OK;
+    };
+    StepVariant<float>* v = nullptr;
+    const int cnt = variant_list(dtype, n, &v);
+    double t = 0;
+    int bc = -1, br = -1;
+    qaf_status s = time_choice(-1, -1, &t);
+    double bt = t;
+    for (int i = 0; i < cnt && s == QAF_OK; ++i) {
+        if (v[i].kind != 0) continue;
+        s = time_choice(i, -1, &t);
+        if (s == QAF_OK && t < bt) { bt = t; bc = i; }
+    }
+    for (int i = 0; i < cnt && s == QAF_OK; ++i) {
+        if (v[i].kind != 1) continue;
+        s = time_choice(bc, i, &t);
+        if (s == QAF_OK && t < bt) { bt = t; br = i; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s != QAF_OK) {
+        set_choice(dtype, n, batched, -1, -1, 0);
+        return s;
+    }
+    set_choice(dtype, n, batched, bc, br, bt);
+    *best_us = bt; *best_col = bc; *best_row = br;
+    return QAF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+qaf_status qaf_autotune(int n, qaf_dtype dtype, int ninst, const char* cache_path, char* choice, int choice_len,
+                        double* us_per_step) {
+    if (!qaf_supported(n, dtype)) return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size");
+    if (ninst < 1) return fail(QAF_ERR_INVALID, "ninst must be >= 1");
+    double us = 0;
+    int col = -1, row = -1;
+    QAF_TRY(dtype == QAF_F64 ? autotune_impl<double>(n, ninst, dtype, &us, &col, &row)
+                             : autotune_impl<float>(n, ninst, dtype, &us, &col, &row));
+    const int batched = ninst > 1 ? 1 : 0;
+    if (us_per_step) *us_per_step = us;
+    if (choice && choice_len > 0) {
+        const std::string c = variant_name(dtype, n, 0, col) + " " + variant_name(dtype, n, 1, row);
+        std::snprintf(choice, (size_t)choice_len, "%s", c.c_str());
+    }
+    if (cache_path && *cache_path) {
+        const std::string dev = device_name();
+        QAF_TRY(cache_write(cache_path, dev, dtype, n, batched, cache_record(dev, dtype, n, batched, col, row, us)));
+    }
+    return QAF_OK;
+}
+
+qaf_status qaf_autotune_load(const char* cache_path) {
+    if (!cache_path) return fail(QAF_ERR_INVALID, "null path");
+    std::ifstream in(cache_path);
+    if (!in) return fail(QAF_ERR_INVALID, std::string("cannot read ") + cache_path);
+    const std::string dev = device_name();
+    std::string line;
+    int used = 0;
+    while (std::getline(in, line)) {
+        std::string d, t, nn, b, c, r, u;
+        if (!(json_field(line, "device", d) && json_field(line, "dtype", t) && json_field(line, "n", nn) &&
+              json_field(line, "batched", b) && json_field(line, "col", c) && json_field(line, "row", r)))
+            continue;
+        if (d != "*" && d != dev) continue;
+        const int dtype = t == "f64" ? QAF_F64 : QAF_F32;
+        const int n = std::atoi(nn.c_str());
+        const int ci = variant_index(dtype, n, 0, c), ri = variant_index(dtype, n, 1, r);
+        if (ci < -1 || ri < -1) continue;   // a variant this build does not have
+        set_choice(dtype, n, std::atoi(b.c_str()) ? 1 : 0, ci, ri, json_field(line, "us_per_step", u) ? std::atof(u.c_str()) : 0);
+        ++used;
+    }
+    (void)used;
+    return QAF_OK;
+}
+
+qaf_status qaf_autotune_reset(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+    return QAF_OK;
+}
+
+qaf_status qaf_set_variant(int n, qaf_dtype dtype, int batched, const char* col, const char* row) {
+    if (!col || !row) return fail(QAF_ERR_INVALID, "null variant name");
+    const int ci = variant_index(dtype, n, 0, col), ri = variant_index(dtype, n, 1, row);
+    if (ci < -1 || ri < -1) return fail(QAF_ERR_INVALID, "unknown launch variant for this size and precision");
+    set_choice(dtype, n, batched ? 1 : 0, ci, ri, 0);
+    return QAF_OK;
+}
+
+qaf_status qaf_variant_choice(int n, qaf_dtype dtype, int batched, char* buf, int len) {
+    if (!buf || len < 1) return fail(QAF_ERR_INVALID, "null buffer");
+    int col = -1, row = -1;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(std::make_tuple((int)dtype, n, batched ? 1 : 0));
+        if (it != g_tune.end()) { col = it->second.col; row = it->second.row; }
+    }
+    const std::string c = variant_name(dtype, n, 0, col) + " " + variant_name(dtype, n, 1, row);
+    std::snprintf(buf, (size_t)len, "%s", c.c_str());
+    return QAF_OK;
+}
+
+qaf_status qaf_variant_list(int n, qaf_dtype dtype, char* buf, int len) {
+    if (!buf || len < 1) return fail(QAF_ERR_INVALID, "null buffer");
+    std::string c = "col:default row:default";
+    StepVariant<float>* v = nullptr;
+    const int cnt = variant_list(dtype, n, &v);
+    for (int i = 0; i < cnt; ++i) c += std::string(" ") + v[i].name;
+    std::snprintf(buf, (size_t)len, "%s", c.c_str());
+    return QAF_OK;
 }
 
 }  // extern "C"

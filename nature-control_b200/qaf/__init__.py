@@ -39,7 +39,8 @@ EXPORTS = [
     "qaf_init_random_q", "qaf_step_noalloc", "qaf_ensemble_create", "qaf_ensemble_destroy",
     "qaf_ensemble_init_random", "qaf_ensemble_load", "qaf_ensemble_store", "qaf_ensemble_advance",
     "qaf_ensemble_diagnostics", "qaf_ensemble_set_controls", "qaf_adjoint_create", "qaf_adjoint_destroy",
-    "qaf_adjoint_forward", "qaf_adjoint_backward",
+    "qaf_adjoint_forward", "qaf_adjoint_backward", "qaf_autotune", "qaf_autotune_load", "qaf_autotune_reset",
+    "qaf_set_variant", "qaf_variant_choice", "qaf_variant_list",
 ]
 
 
@@ -142,6 +143,13 @@ def lib():
         L.qaf_adjoint_destroy.argtypes = [vp]
         L.qaf_adjoint_forward.argtypes = [vp, ctypes.POINTER(CParams), vp, vp, vp, vp, vp, vp, dp, vp]
         L.qaf_adjoint_backward.argtypes = [vp, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp, vp]
+        sp = ctypes.c_char_p
+        L.qaf_autotune.argtypes = [cp, cp, cp, sp, sp, cp, dp]
+        L.qaf_autotune_load.argtypes = [sp]
+        L.qaf_autotune_reset.argtypes = []
+        L.qaf_set_variant.argtypes = [cp, cp, cp, sp, sp]
+        L.qaf_variant_choice.argtypes = [cp, cp, cp, sp, cp]
+        L.qaf_variant_list.argtypes = [cp, cp, sp, cp]
         _lib = L
     return _lib
 
@@ -160,6 +168,41 @@ def version() -> str:
 
 def supported(n: int, dtype: int = F32) -> bool:
     return bool(lib().qaf_supported(n, dtype))
+
+
+def autotune(n: int, dtype: int = F32, ninst: int = 1, cache: Optional[str] = None):
+    """Time the launch shapes of the fused step kernels for n x n on `ninst`
+    synthetic instances and keep the fastest; returns (choice, us per step)."""
+    buf = ctypes.create_string_buffer(128)
+    us = ctypes.c_double()
+    _check(lib().qaf_autotune(n, dtype, ninst, cache.encode() if cache else None, buf, 128, ctypes.byref(us)))
+    return buf.value.decode(), us.value
+
+
+def autotune_load(path: str):
+    """Apply the records of an autotuner cache that match this GPU."""
+    _check(lib().qaf_autotune_load(path.encode()))
+
+
+def autotune_reset():
+    """Back to the built-in launch shapes."""
+    _check(lib().qaf_autotune_reset())
+
+
+def set_variant(n: int, dtype: int, batched: bool, col: str = "default", row: str = "default"):
+    _check(lib().qaf_set_variant(n, dtype, 1 if batched else 0, col.encode(), row.encode()))
+
+
+def variant_choice(n: int, dtype: int = F32, batched: bool = False) -> str:
+    buf = ctypes.create_string_buffer(128)
+    _check(lib().qaf_variant_choice(n, dtype, 1 if batched else 0, buf, 128))
+    return buf.value.decode()
+
+
+def variant_list(n: int, dtype: int = F32):
+    buf = ctypes.create_string_buffer(512)
+    _check(lib().qaf_variant_list(n, dtype, buf, 512))
+    return buf.value.decode().split()
 
 
 def _stream():
@@ -373,8 +416,21 @@ class Ensemble:
     """
 
     def __init__(self, n, p: Params, alpha, rf=None, lx: float = 2 * math.pi, ly: Optional[float] = None,
-                 dtype: int = F32):
+                 dtype: int = F32, tune: bool = False, tune_cache: Optional[str] = None):
+        """tune: time the launch shapes for each grid size first (tune_cache:
+        read the choices from this JSON-lines file when it has them, else tune
+        and record them there)."""
         self.n = [int(v) for v in n]
+        if tune_cache is not None and os.path.exists(tune_cache):
+            autotune_load(tune_cache)
+        if tune:
+            for size in sorted(set(self.n)):
+                count = self.n.count(size)
+                if tune_cache is not None and os.path.exists(tune_cache) and \
+                        variant_choice(size, dtype, count > 1) != "col:default row:default":
+                    continue
+                autotune(size, dtype, count, tune_cache)
+        self.tuned = {size: variant_choice(size, dtype, self.n.count(size) > 1) for size in sorted(set(self.n))}
         k = len(self.n)
         self.alpha = [float(v) for v in alpha]
         self.rf = [float(p.rf)] * k if rf is None else [float(v) for v in rf]
