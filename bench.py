@@ -1,7 +1,7 @@
 """Throughput benchmark of the IF-RK4 pseudo-spectral step (w, r1, r2).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl qaf|reference] [--dtype f32|f64]
-                    [--workload plain|ensemble|adjoint]
+                    [--workload plain|ensemble|adjoint|control]
 
 Workload: the "plain throughput" configuration — 1024 x 1024 periodic grid,
 L = 16 pi, friction solver parameters Re = 1 (nu = 1), Rf = 0.1 (mu = 0.1),
@@ -40,6 +40,14 @@ the whole horizon (--steps is capped at 5, 3 warm-up passes). `value` is
 (adjoint + recompute time) / (plain forward time); also reported: the
 directional derivatives of the FP32 and FP64 adjoint gradients against
 central differences of the FP64 forward on 16 random directions.
+
+--workload control: the batched forward + adjoint control loop — 64
+instances of 256 x 256 FP32, each with its own activity field Ra_k(x) as
+above (seeds 100..163) and its own seeded initial Q, 1000-step horizon,
+gradient descent on each instance's terminal enstrophy. A bench step is one
+gradient-descent iteration of all 64 instances (forward, recompute + adjoint,
+update). `value`: instance-iterations per second; `looped`: one instance's
+iteration through the single-instance adjoint, times 64.
 """
 from __future__ import annotations
 
@@ -67,6 +75,8 @@ ENS_DT = 1e-3
 ENS_METRIC = "sum_i N_i^2*steps/s, 256-instance mixed-size ensemble, IF-RK4"
 ADJ_N, ADJ_STEPS, ADJ_DT, ADJ_K, ADJ_WINDOW, ADJ_SEED = 256, 2000, 1e-3, 64, 100, 2
 ADJ_METRIC = "(adjoint + recompute) time / forward time, 256^2 FP32, 2000 IF-RK4 steps, K=64"
+CTL_N, CTL_INST, CTL_STEPS, CTL_K, CTL_LR = 256, 64, 1000, 50, 0.05
+CTL_METRIC = "gradient-descent instance-iterations/s, 64 x 256^2 FP32, 1000-step horizon, terminal enstrophy"
 
 
 def parse():
@@ -79,7 +89,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
-    ap.add_argument("--workload", choices=["plain", "ensemble", "adjoint"], default="plain")
+    ap.add_argument("--workload", choices=["plain", "ensemble", "adjoint", "control"], default="plain")
+    ap.add_argument("--horizon", type=int, default=CTL_STEPS, help="control workload: steps per rollout")
     ap.add_argument("--no-fd", action="store_true", help="adjoint workload: skip the finite-difference check")
     ap.add_argument("--no-tune", action="store_true", help="ensemble workload: keep the built-in launch shapes")
     ap.add_argument("--instances", type=int, default=ENS_COUNT)
@@ -701,6 +712,89 @@ def adjoint_cpu_baseline(n, dt, alpha_np):
                       f"tangent-linear {tt*1e3:.1f} ms/step (one directional derivative per pass)"}
 
 
+def run_control(a, world, rank, local):
+    import numpy as np
+    import torch
+
+    import qaf
+
+    n, ni, T, K, lr = CTL_N, CTL_INST, a.horizon, min(CTL_K, a.horizon), CTL_LR
+    iters, warm = max(1, min(a.steps, 5)), 1
+    p = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=ADJ_DT, q_lin=1.0, advect_omega=1)
+    batch = qaf.AdjointBatch(ni, n, p, T, K, 1, lx=L, dtype=qaf.F32)
+    mesh = batch.mesh
+    alpha = torch.stack([torch.as_tensor(smoothed_alpha(n, 100 + k), dtype=torch.float32) for k in range(ni)]).cuda()
+    st = [mesh.random_q(100 + k) for k in range(ni)]
+    s0 = [torch.stack([st[k][f] for k in range(ni)]).contiguous() for f in range(3)]
+    history = []
+
+    def iteration():
+        nonlocal alpha
+        losses, _ = batch.forward(*s0, alpha=alpha, final_state=False)
+        _, _, _, ga = batch.backward(None, [1.0] * ni)
+        scale = ga.abs().amax(dim=(1, 2), keepdim=True).clamp_min(1e-30)
+        alpha = (alpha - lr * ga / scale).contiguous()       # normalised descent step per instance
+        return losses
+
+    for _ in range(warm):
+        history.append(iteration())
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()
+        for _ in range(iters):
+            history.append(iteration())
+        e1.record()
+        torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world) / iters
+    final, _ = batch.forward(*s0, alpha=alpha, final_state=False)
+    history.append(final)
+    value = world * ni / (ms * 1e-3)
+
+    # looped: the same iteration for one instance through the single-instance adjoint, times 64
+    single = qaf.Adjoint(qaf.Mesh(n, lx=L, dtype=qaf.F32), T, K, 1)
+    ps = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=ADJ_DT, q_lin=1.0, advect_omega=1)
+    ps.alpha_field = alpha[0].contiguous()
+    for _ in range(2):
+        single.forward(ps, *st[0], final_state=False)
+        single.backward(None, 1.0)
+    e0.record()
+    single.forward(ps, *st[0], final_state=False)
+    single.backward(None, 1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_single = e0.elapsed_time(e1)
+    looped = 1.0 / (ms_single * 1e-3)
+
+    ca = (n // 2 + 1) * n * 2 * 4
+    pr = n * n * 4
+    bytes_iter = ni * T * (4 * 55 * ca + 4 * (55 * ca + 9 * pr) + 4 * ((9 + 11 + 9) * ca + (11 + 9) * ca + (9 + 2) * pr))
+    peak, peak_kind = peaks()
+    achieved = bytes_iter / (ms * 1e-3) / 1e9
+    l0 = np.mean(history[0])
+    lN = np.mean(history[-1])
+    return {
+        "metric": CTL_METRIC, "value": value, "unit": "instance-iterations/s", "n_gpus": world, "steps": iters,
+        "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded random Q per instance; seeded smoothed activity fields)",
+        "config": {"workload": f"control loop: {ni} x {n}^2 FP32, horizon {T} IF-RK4 steps dt={ADJ_DT}, Ra_k(x) = "
+                               f"1 + 0.1 smoothed N(0,1) (seeds 100..{100 + ni - 1}), loss = terminal enstrophy, "
+                               f"checkpoints every {K} steps, normalised descent step {lr}",
+                   "instances": ni, "grid": n, "horizon": T, "parallelism": f"replicas x{world}",
+                   "l2": f"recording of a segment ({ni * K * 4 * 9 * pr / 1e9:.0f} GB) larger than L2"},
+        "loss_mean_first": l0, "loss_mean_last": lN, "loss_history_mean": [float(np.mean(h)) for h in history],
+        "looped": {"value": looped, "unit": "instance-iterations/s", "ms_per_instance_iteration": ms_single,
+                   "what": "one instance's iteration through the single-instance adjoint (qaf_adjoint_*); 64 such run one after another"},
+        "roofline": {"bound": "hbm", "kernel": "one iteration (forward, recompute, adjoint) of the batch",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_step": bytes_iter},
+        "e2e": {"value": value, "unit": "instance-iterations/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": ni * 8},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+    }
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -709,7 +803,7 @@ def main():
         if rank == 0:
             if a.workload == "ensemble":
                 line = run_reference_ensemble(a)
-            elif a.workload == "adjoint":
+            elif a.workload in ("adjoint", "control"):
                 line = {"impl": "reference", "unavailable": "the reference computes no gradients (no adjoint or "
                                                             "tangent model anywhere in it)"}
             else:
@@ -723,6 +817,8 @@ def main():
         line = run_ensemble(a, world, rank, local)
     elif a.workload == "adjoint":
         line = run_adjoint(a, world, rank, local)
+    elif a.workload == "control":
+        line = run_control(a, world, rank, local)
     else:
         line = run_qaf(a, world, rank, local)
     if rank == 0:

@@ -245,6 +245,25 @@ qaf_status qaf_adjoint_forward(qaf_adjoint* adj, const qaf_params* p, const void
 qaf_status qaf_adjoint_backward(qaf_adjoint* adj, const void* gwT, const void* gr1T, const void* gr2T, double gloss,
                                 void* gw0, void* gr1_0, void* gr2_0, void* galpha, void* stream);
 
+/* ---- batched adjoint -----------------------------------------------------------
+ * No counterpart in the reference. `ninst` instances of one grid size (n <= 256)
+ * sharing the parameters p (fixed at creation) but each with its own initial
+ * spectra and activity field, stepped and differentiated together: every stage
+ * of the forward, the recompute and the adjoint is one launch for the batch.
+ * Arrays hold the instances back to back: spectra [ninst][ny][nx/2+1],
+ * activity fields and their gradients [ninst][ny][nx]. losses[k] (host) is
+ * instance k's mean enstrophy over the last loss_window states; glosses[k]
+ * (host, NULL: zero) its weight in the objective. */
+typedef struct qaf_adjoint_batch qaf_adjoint_batch;
+qaf_status qaf_adjoint_batch_create(int ninst, int n, double lx, double ly, qaf_dtype dtype, const qaf_params* p,
+                                    int nsteps, int checkpoint_every, int loss_window, qaf_adjoint_batch** out);
+qaf_status qaf_adjoint_batch_destroy(qaf_adjoint_batch* batch);
+qaf_status qaf_adjoint_batch_forward(qaf_adjoint_batch* batch, const void* w0, const void* r1_0, const void* r2_0,
+                                     const void* alpha, void* wT, void* r1T, void* r2T, double* losses, void* stream);
+qaf_status qaf_adjoint_batch_backward(qaf_adjoint_batch* batch, const void* gwT, const void* gr1T, const void* gr2T,
+                                      const double* glosses, void* gw0, void* gr1_0, void* gr2_0, void* galpha,
+                                      void* stream);
+
 /* ---- allocation-free step --------------------------------------------------
  * No counterpart in the reference (whose Mesh and Field always cudaMalloc).
  * For callers that cannot allocate device memory when they step — work

@@ -62,12 +62,21 @@ struct AdjArgs {
     cplx<real>* edge;          // 6 * N scratch: kb of the kx = 0 and kx = N/2 columns
     const cplx<real>* wstate;  // w of the state whose adjoint completes in this launch (loss term) or nullptr
     real loss_w;               // d loss / d enstrophy of that state
+    const real* loss_wv;       // per instance instead of loss_w, or nullptr
     int stage;                 // 4..1: Tx holds the transposed products of this stage; 0: start from sbar
     int emit;                  // write Tg for the stage before
     const real* phys;          // the stage input's forward fields (PhysField order, N*N each)
     const real* alpha_field;   // activity field or nullptr (alpha)
     real alpha;
     real* alpha_grad;          // += d loss / d alpha(x), or nullptr
+    // batches of instances (field-parallel kernels): instance k's data at these offsets
+    int ninst;                 // instances in the launch (1: a single grid)
+    size_t s_istride;          // complex elements: abar, sacc, sbar, wstate
+    size_t tg_istride;         // complex elements: Tg
+    size_t tx_istride;         // complex elements: Tx
+    size_t p_istride;          // reals: phys
+    size_t a_istride;          // reals: alpha_field (0: one field for all)
+    size_t g_istride;          // reals: alpha_grad
 };
 
 // conj(multiplier) of the forward field p (derived()) applied to the transform of its adjoint
@@ -363,12 +372,19 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
     XchgCols<real> x{buf, w, W};
     TeamFFT<real, N, E> fft;
     fft.template init<N>(t, a.tw);
-    const bool edge = blockIdx.x == gridDim.x - 1;
+    constexpr int BPI = H / W + 1;                 // CTAs per instance: H/W column blocks + the edge CTA
+    const int inst = blockIdx.x / BPI, lb = blockIdx.x % BPI;
+    const size_t so = a.s_istride * inst;
+    const cplx<real>* Tx = a.Tx + a.tx_istride * inst;
+    cplx<real>* Tg = a.Tg + a.tg_istride * inst;
+    const cplx<real>* wst = a.wstate ? a.wstate + so : nullptr;
+    const bool edge = lb == BPI - 1;
+    const real lw = a.loss_wv ? a.loss_wv[inst] : a.loss_w;
     const bool emit_q = f < NGA && (a.advect || f > GA_VW);
     const real n2 = (real)1 / ((real)N * (real)N);
 
     if (!edge) {
-        const int i = blockIdx.x * W + w;
+        const int i = lb * W + w;
         const bool active = i != 0;
         const real kx = a.dkx * (real)i;
         if (a.stage >= 1) {
@@ -376,7 +392,7 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
             cplx<real> v[E];
 #pragma unroll
             for (int e = 0; e < E; ++e)
-                v[e] = mine ? a.Tx[(size_t)f * N * H + (size_t)(t + TEAM * e) * H + i] : mk<real>(0, 0);
+                v[e] = mine ? Tx[(size_t)f * N * H + (size_t)(t + TEAM * e) * H + i] : mk<real>(0, 0);
             fft.template run<false>(t, v, x);
             if (f < PF_COUNT)
 #pragma unroll
@@ -389,7 +405,7 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
         }
         __syncthreads();
         for (int pt = tid; pt < N * W; pt += NTH) {
-            const int j = pt / W, w2 = pt % W, i2 = blockIdx.x * W + w2;
+            const int j = pt / W, w2 = pt % W, i2 = lb * W + w2;
             if (i2 == 0) continue;
             cplx<real> cb[3] = {mk<real>(0, 0), mk<real>(0, 0), mk<real>(0, 0)};
             if (a.stage >= 1)
@@ -397,13 +413,13 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
                 for (int p = 0; p < PF_COUNT; ++p) cb[adj_target(p)] = cadd(cb[adj_target(p)], sm[(size_t)p * SPAN + j * W + w2]);
             const size_t idx = (size_t)j * NXH + i2;
             const bool keep = adj_keep(a, i2, j);
-            const cplx<real> lossg = a.wstate ? cscale(a.wstate[idx], 2 * a.loss_w * n2 * n2) : mk<real>(0, 0);
+            const cplx<real> lossg = wst ? cscale(wst[idx], 2 * lw * n2 * n2) : mk<real>(0, 0);
 #pragma unroll
             for (int g = 0; g < 3; ++g) {
                 real Ef, Eh;
                 adj_factors<real, N>(a, g, i2, j, Ef, Eh);
                 sm[(size_t)g * SPAN + j * W + w2] =
-                    adj_rk(a, g, idx, cscale(cb[g], 2 * n2), Ef, Eh, keep, g == 0 ? lossg : mk<real>(0, 0));
+                    adj_rk(a, g, so + idx, cscale(cb[g], 2 * n2), Ef, Eh, keep, g == 0 ? lossg : mk<real>(0, 0));
             }
         }
         __syncthreads();
@@ -422,7 +438,7 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
         fft.template run<true>(t, v, x);
         if (emit_q && active)
 #pragma unroll
-            for (int e = 0; e < E; ++e) a.Tg[(size_t)f * N * H + (size_t)(t + TEAM * e) * H + i] = v[e];
+            for (int e = 0; e < E; ++e) Tg[(size_t)f * N * H + (size_t)(t + TEAM * e) * H + i] = v[e];
         return;
     }
 
@@ -433,7 +449,7 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
         const bool mine = f < PF_COUNT && lead && a.stage >= 1;
         cplx<real> v[E];
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = mine ? a.Tx[(size_t)f * N * H + (size_t)(t + TEAM * e) * H] : mk<real>(0, 0);
+        for (int e = 0; e < E; ++e) v[e] = mine ? Tx[(size_t)f * N * H + (size_t)(t + TEAM * e) * H] : mk<real>(0, 0);
         fft.template run<false>(t, v, x);
         if (lead)
 #pragma unroll
@@ -464,9 +480,9 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
         for (int p = 0; p < PF_COUNT; ++p) cb[adj_target(p)] = cadd(cb[adj_target(p)], sm[(size_t)p * SPAN + c * N + j]);
         const size_t idx = (size_t)j * NXH + i;
         cplx<real> lossg = mk<real>(0, 0);
-        if (a.wstate) {
-            const cplx<real> P = cscale(cadd(a.wstate[idx], cconj(a.wstate[(size_t)jm * NXH + i])), (real)0.5);
-            lossg = cscale(P, a.loss_w * n2 * n2);
+        if (wst) {
+            const cplx<real> P = cscale(cadd(wst[idx], cconj(wst[(size_t)jm * NXH + i])), (real)0.5);
+            lossg = cscale(P, lw * n2 * n2);
         }
         const bool keep = adj_keep(a, i, j);
 #pragma unroll
@@ -474,7 +490,7 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
             real Ef, Eh;
             adj_factors<real, N>(a, g, i, j, Ef, Eh);
             sm[(size_t)g * SPAN + c * N + j] =
-                adj_rk(a, g, idx, cscale(cb[g], n2), Ef, Eh, keep, g == 0 ? lossg : mk<real>(0, 0));
+                adj_rk(a, g, so + idx, cscale(cb[g], n2), Ef, Eh, keep, g == 0 ? lossg : mk<real>(0, 0));
         }
     }
     __syncthreads();
@@ -506,7 +522,7 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
     fft.template run<true>(t, v, x);
     if (emit_q && lead)
 #pragma unroll
-        for (int e = 0; e < E; ++e) a.Tg[(size_t)f * N * H + (size_t)(t + TEAM * e) * H] = v[e];
+        for (int e = 0; e < E; ++e) Tg[(size_t)f * N * H + (size_t)(t + TEAM * e) * H] = v[e];
 }
 
 // Field-parallel row kernel: one team of H/E threads per (transform, row),
@@ -521,7 +537,12 @@ __global__ void __launch_bounds__(NGA * (N / 2 / E)) adj_row_kernel(const __grid
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<real>* sm = reinterpret_cast<cplx<real>*>(smem_raw);
     const int q = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
-    const int n = blockIdx.x;
+    const int inst = blockIdx.x / N, n = blockIdx.x % N;
+    const cplx<real>* Tg = a.Tg + a.tg_istride * inst;
+    cplx<real>* Tx = a.Tx + a.tx_istride * inst;
+    const real* phys = a.phys + a.p_istride * inst;
+    const real* alf = a.alpha_field ? a.alpha_field + a.a_istride * inst : nullptr;
+    real* agr = a.alpha_grad ? a.alpha_grad + a.g_istride * inst : nullptr;
     cplx<real>* buf = sm + (size_t)q * H;
     real* row = reinterpret_cast<real*>(buf);
     const real* rows = reinterpret_cast<const real*>(sm);   // field q at rows[q * N + x]
@@ -532,7 +553,7 @@ __global__ void __launch_bounds__(NGA * (N / 2 / E)) adj_row_kernel(const __grid
 
     // 1. g_q = C2R of row n of Tg[q] (slot 0 of a T row holds DC + i Nyquist)
     {
-        const cplx<real>* tr = a.Tg + (size_t)q * N * H + (size_t)n * H;
+        const cplx<real>* tr = Tg + (size_t)q * N * H + (size_t)n * H;
         cplx<real> v[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
@@ -563,10 +584,10 @@ __global__ void __launch_bounds__(NGA * (N / 2 / E)) adj_row_kernel(const __grid
     real* rw = reinterpret_cast<real*>(sm);
     for (int xi = threadIdx.x; xi < N; xi += TPR) {
         const size_t pi = (size_t)n * N + xi;
-        const real w = a.phys[PF_W * NN + pi], r1 = a.phys[PF_R1 * NN + pi], r2 = a.phys[PF_R2 * NN + pi];
-        const real u = a.phys[PF_U * NN + pi], v = a.phys[PF_V * NN + pi], ux = a.phys[PF_UX * NN + pi];
-        const real sh = a.phys[PF_SH * NN + pi], L1 = a.phys[PF_LR1 * NN + pi], L2 = a.phys[PF_LR2 * NN + pi];
-        const real al = a.alpha_field ? a.alpha_field[pi] : a.alpha;
+        const real w = phys[PF_W * NN + pi], r1 = phys[PF_R1 * NN + pi], r2 = phys[PF_R2 * NN + pi];
+        const real u = phys[PF_U * NN + pi], v = phys[PF_V * NN + pi], ux = phys[PF_UX * NN + pi];
+        const real sh = phys[PF_SH * NN + pi], L1 = phys[PF_LR1 * NN + pi], L2 = phys[PF_LR2 * NN + pi];
+        const real al = alf ? alf[pi] : a.alpha;
         real g[NGA];
 #pragma unroll
         for (int k = 0; k < NGA; ++k) g[k] = rows[k * N + xi];
@@ -577,7 +598,7 @@ __global__ void __launch_bounds__(NGA * (N / 2 / E)) adj_row_kernel(const __grid
         const real Sb = (-lam * L1 + dsgl * r1) * g[GA_P11] + (-lam * L2 + dsgl * r2) * g1221 +
                         (-2 * S * r1 + lam * ux) * g[GA_A1] + (-2 * S * r2 + (real)0.5 * lam * sh) * g[GA_A2];
         const real dS1 = S > 0 ? 4 * r1 / S : (real)0, dS2 = S > 0 ? 4 * r2 / S : (real)0;
-        if (a.alpha_grad) a.alpha_grad[pi] += -(r1 * g[GA_P11] + r2 * g1221);
+        if (agr) agr[pi] += -(r1 * g[GA_P11] + r2 * g1221);
         rw[PF_W * N + xi] = -u * g[GA_UW] - v * g[GA_VW] - r2 * g[GA_A1] + r1 * g[GA_A2];
         rw[PF_R1 * N + xi] = (sgl - al) * g[GA_P11] - 2 * L2 * g[GA_P12] + 2 * L2 * g[GA_P21] - S * S * g[GA_A1] -
                              u * g[GA_UR1] - v * g[GA_VR1] + w * g[GA_A2] + Sb * dS1;
@@ -605,7 +626,7 @@ __global__ void __launch_bounds__(NGA * (N / 2 / E)) adj_row_kernel(const __grid
     for (int e = 0; e < E; ++e) x.write(t + TEAM * e, v[e]);
     x.sync();
     if (q < PF_COUNT) {
-        cplx<real>* out = a.Tx + (size_t)q * N * H + (size_t)n * H;
+        cplx<real>* out = Tx + (size_t)q * N * H + (size_t)n * H;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int k = t + TEAM * e;
@@ -624,6 +645,11 @@ __global__ void __launch_bounds__(NGA * (N / 2 / E)) adj_row_kernel(const __grid
 // loss += weight * (0.5 / N^4) * diag[0] (the enstrophy sum of the step's new state); weight carries 1/N^4
 __global__ void adj_loss_accumulate(const double* diag, double* loss, double weight) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *loss += weight * 0.5 * diag[0];
+}
+// the same for ninst instances (diag: 2 doubles per instance)
+__global__ void adj_loss_accumulate_batch(const double* diag, double* loss, double weight, int ninst) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < ninst) loss[k] += weight * 0.5 * diag[2 * k];
 }
 
 }  // namespace qaf

@@ -1155,6 +1155,7 @@ struct EnsGroup {
     real* inst_alpha = nullptr;
     real* inst_e0 = nullptr;
     double* diag = nullptr;         // 2 per instance
+    real* alpha_fields = nullptr;   // per-instance activity fields (N*N each), or nullptr: inst_alpha
 };
 
 // per-instance buffer layout (complex elements), returned size rounded up to
@@ -1236,6 +1237,7 @@ StageArgs<real> group_args(const qaf_ensemble* e, const EnsGroup<real>& g) {
     a.flags = g.w.flags; a.queue = g.w.queue; a.tm_G = g.w.tm_G;
     a.ninst = g.ninst; a.istride = g.istride;
     a.inst_alpha = g.inst_alpha; a.inst_e0 = g.inst_e0;
+    if (g.alpha_fields) { a.alpha_field = g.alpha_fields; a.alpha_istride = (size_t)N * N; }
     a.diag = g.diag; a.diag_istride = 2;
     a.integrator = INT_IFRK4;
     return a;
@@ -1748,6 +1750,7 @@ struct OpAdjBackward {
         a.alpha_field = reinterpret_cast<const real*>(A->p.alpha_field);
         a.alpha = (real)A->p.alpha;
         a.alpha_grad = reinterpret_cast<real*>(A->agrad);
+        a.ninst = 1;
         const real lw = (real)(A->window > 0 ? gloss / A->window : 0.0);
         a.loss_w = lw;
 
@@ -2146,3 +2149,332 @@ qaf_status qaf_variant_list(int n, qaf_dtype dtype, char* buf, int len) {
 
 }  // extern "C"
 
+// ===========================================================================
+// Batched adjoint: `ninst` instances of one grid size, each with its own
+// initial state and activity field, advanced and differentiated together —
+// every forward, recompute and adjoint stage is one launch for the whole
+// batch (the ensemble's instance-indexed kernels and the instance-indexed
+// field-parallel adjoint kernels). Grids up to 256 x 256.
+// ===========================================================================
+struct qaf_adjoint_batch {
+    qaf_ensemble* ens = nullptr;    // ninst instances of size n: forward machinery and tables
+    int ninst = 0, n = 0, nsteps = 0, K = 0, window = 0, nseg = 0;
+    size_t ns = 0, np = 0;
+    unsigned char* blk = nullptr;
+    unsigned char *ckpt = nullptr, *wlog = nullptr, *phys = nullptr, *Tg = nullptr, *Tx = nullptr;
+    unsigned char *abar = nullptr, *sacc = nullptr, *sbar = nullptr, *agrad = nullptr, *alpha = nullptr, *lossw = nullptr;
+    double* loss = nullptr;
+    bool have_alpha = false, have_forward = false;
+};
+
+namespace {
+
+// spectral arrays of the batch: [field][instance][ns]
+template <typename real>
+cplx<real>* bfield(unsigned char* base, size_t ns, int ninst, int f) {
+    return reinterpret_cast<cplx<real>*>(base) + (size_t)f * ninst * ns;
+}
+
+template <typename real>
+struct BatchOps {
+    static EnsGroup<real>& group(qaf_adjoint_batch* B) { return groups<real>(B->ens)[0]; }
+
+    // load field-major [field][inst][ns] reference-layout spectra into the group's states
+    static qaf_status load(qaf_adjoint_batch* B, const cplx<real>* const* src, size_t src_istride, cudaStream_t st) {
+        EnsGroup<real>& g = group(B);
+        dim3 grid(grid_for(B->ns), B->ninst);
+        for (int f = 0; f < 3; ++f)
+            ref_to_internal_batch<real><<<grid, 256, 0, st>>>(src[f], src_istride, g.w.old_m[f], g.w.old_n[f], g.istride, B->n);
+        B->ens->y_valid = false;
+        return post_launch("adjoint batch load");
+    }
+    static qaf_status store(qaf_adjoint_batch* B, cplx<real>* const* dst, size_t dst_istride, cudaStream_t st) {
+        EnsGroup<real>& g = group(B);
+        dim3 grid(grid_for(B->ns), B->ninst);
+        for (int f = 0; f < 3; ++f)
+            internal_to_ref_batch<real><<<grid, 256, 0, st>>>(g.w.old_m[f], g.w.old_n[f], g.istride, dst[f], dst_istride, B->n);
+        return post_launch("adjoint batch store");
+    }
+
+    // nsteps IF-RK4 steps of the whole batch, recording on request the stage inputs' fields
+    // (phys: per step and stage ninst * PF_COUNT * N * N reals), w after the steps from local
+    // step wfrom on (wlog: ninst spectra per step, indexed from wfrom) and the loss
+    template <int N>
+    static qaf_status advance(qaf_adjoint_batch* B, int nsteps, real* phys, cplx<real>* wlog, int wfrom, bool loss,
+                              int loss_from, double lweight, cudaStream_t st) {
+        qaf_ensemble* e = B->ens;
+        EnsGroup<real>& g = group(B);
+        if (!e->y_valid) {
+            QAF_TRY(ens_prologue<real>(e, st));
+            e->y_valid = true;
+        }
+        StageArgs<real> a = group_args<real>(e, g);
+        a.mode = MODE_STAGE;
+        a.do_inverse = 1;
+        a.phys_istride = (size_t)PF_COUNT * N * N;
+        const size_t slot = (size_t)B->ninst * PF_COUNT * N * N;
+        for (int s = 0; s < nsteps; ++s) {
+            const bool lstep = loss && s >= loss_from;
+            if (lstep) QAF_CUDA(cudaMemsetAsync(g.diag, 0, 2 * (size_t)B->ninst * sizeof(double), st));
+            for (int k = 1; k <= 4; ++k) {
+                a.stage = k;
+                a.last_stage = k == 4;
+                a.diag = (lstep && k == 4) ? g.diag : nullptr;
+                a.phys_out = phys ? phys + ((size_t)s * 4 + (k - 1)) * slot : nullptr;
+                Launch<real, N>::row(a, st);
+                Launch<real, N>::col(a, st);
+            }
+            if (lstep) adj_loss_accumulate_batch<<<(B->ninst + 127) / 128, 128, 0, st>>>(g.diag, B->loss, lweight, B->ninst);
+            if (wlog && s >= wfrom) {
+                dim3 grid(grid_for(B->ns), B->ninst);
+                internal_to_ref_batch<real><<<grid, 256, 0, st>>>(g.w.old_m[0], g.w.old_n[0], g.istride,
+                                                                  wlog + (size_t)(s - wfrom) * B->ninst * B->ns, B->ns, N);
+            }
+        }
+        return post_launch("adjoint batch advance");
+    }
+};
+
+template <typename real, int N>
+qaf_status batch_forward(qaf_adjoint_batch* B, const void* const* s0, const void* alpha, void* const* sT, double* losses,
+                         cudaStream_t st) {
+    using O = BatchOps<real>;
+    EnsGroup<real>& g = O::group(B);
+    const size_t ns = B->ns, cb = sizeof(cplx<real>), ni = (size_t)B->ninst;
+    if (alpha) {
+        QAF_CUDA(cudaMemcpyAsync(B->alpha, alpha, ni * N * N * sizeof(real), cudaMemcpyDeviceToDevice, st));
+        g.alpha_fields = reinterpret_cast<real*>(B->alpha);
+        B->have_alpha = true;
+    } else {
+        g.alpha_fields = nullptr;
+        B->have_alpha = false;
+    }
+    for (int f = 0; f < 3; ++f)   // checkpoint 0: the inputs
+        QAF_CUDA(cudaMemcpyAsync(bfield<real>(B->ckpt, ns, B->ninst, f), s0[f], ni * ns * cb, cudaMemcpyDeviceToDevice, st));
+    const cplx<real>* src[3] = {bfield<real>(B->ckpt, ns, B->ninst, 0), bfield<real>(B->ckpt, ns, B->ninst, 1),
+                                bfield<real>(B->ckpt, ns, B->ninst, 2)};
+    QAF_TRY(O::load(B, src, ns, st));
+    QAF_CUDA(cudaMemsetAsync(B->loss, 0, ni * sizeof(double), st));
+    const double n4 = (double)N * N * (double)N * N;
+    const double lweight = 1.0 / ((double)(B->window > 0 ? B->window : 1) * n4);
+    for (int seg = 0; seg < B->nseg; ++seg) {
+        const int t0 = seg * B->K, t1 = std::min(B->nsteps, t0 + B->K);
+        QAF_TRY(O::template advance<N>(B, t1 - t0, nullptr, nullptr, 0, B->window > 0, B->nsteps - B->window - t0,
+                                       lweight, st));
+        if (t1 < B->nsteps) {
+            unsigned char* c = B->ckpt + (size_t)(seg + 1) * 3 * ni * ns * cb;
+            cplx<real>* dst[3] = {bfield<real>(c, ns, B->ninst, 0), bfield<real>(c, ns, B->ninst, 1),
+                                  bfield<real>(c, ns, B->ninst, 2)};
+            QAF_TRY(O::store(B, dst, ns, st));
+        }
+    }
+    if (sT[0] && sT[1] && sT[2]) {
+        cplx<real>* dst[3] = {static_cast<cplx<real>*>(sT[0]), static_cast<cplx<real>*>(sT[1]),
+                              static_cast<cplx<real>*>(sT[2])};
+        QAF_TRY(O::store(B, dst, ns, st));
+    }
+    if (losses) {
+        QAF_CUDA(cudaMemcpyAsync(losses, B->loss, ni * sizeof(double), cudaMemcpyDeviceToHost, st));
+        QAF_CUDA(cudaStreamSynchronize(st));
+    }
+    return post_launch("qaf_adjoint_batch_forward");
+}
+
+template <typename real, int N>
+qaf_status batch_backward(qaf_adjoint_batch* B, const void* const* gT, const double* glosses, void* const* g0,
+                          void* galpha, cudaStream_t st) {
+    using O = BatchOps<real>;
+    constexpr int H = N / 2;
+    constexpr int W = 1, EC = N / 16 > 4 ? N / 16 : 4;
+    constexpr int COL_THREADS = NGA * W * (N / EC);
+    constexpr size_t COL_SMEM = (size_t)NGA * N * 2 * sizeof(cplx<real>);
+    constexpr int ER = H / 16 < 2 ? 2 : (H / 16 > 16 ? 16 : H / 16);
+    constexpr int ROW_THREADS = NGA * (H / ER);
+    constexpr size_t ROW_SMEM = (size_t)NGA * H * sizeof(cplx<real>);
+    static bool attrs = false;
+    if (!attrs) {
+        QAF_CUDA(cudaFuncSetAttribute(adj_colp_kernel<real, N, W, EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COL_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(adj_row_kernel<real, N, ER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROW_SMEM));
+        attrs = true;
+    }
+    qaf_ensemble* e = B->ens;
+    EnsGroup<real>& g = O::group(B);
+    const size_t ns = B->ns, cb = sizeof(cplx<real>), ni = (size_t)B->ninst;
+    const qaf_params& p = e->p;
+    AdjArgs<real> a;
+    std::memset(&a, 0, sizeof(a));
+    a.dkx = (real)(2 * M_PI / e->lx); a.dky = (real)(2 * M_PI / e->ly); a.dt = (real)p.dt; a.lambda = (real)p.lambda;
+    a.ce = (real)(1.0 / (p.er * p.re));
+    a.advect = p.advect_omega ? 1 : 0;
+    a.kx_keep = H * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
+    a.tw = g.w.tw; a.ex = g.w.ex; a.ey = g.w.ey;
+    host_if_e0<real>(p.dt, p.re, p.rf, p.q_lin, a.e0);
+    a.Tg = reinterpret_cast<cplx<real>*>(B->Tg); a.Tx = reinterpret_cast<cplx<real>*>(B->Tx);
+    for (int f = 0; f < 3; ++f) {
+        a.abar[f] = bfield<real>(B->abar, ns, B->ninst, f);
+        a.sacc[f] = bfield<real>(B->sacc, ns, B->ninst, f);
+        a.sbar[f] = bfield<real>(B->sbar, ns, B->ninst, f);
+    }
+    a.alpha_field = B->have_alpha ? reinterpret_cast<const real*>(B->alpha) : nullptr;
+    a.alpha = (real)p.alpha;
+    a.alpha_grad = reinterpret_cast<real*>(B->agrad);
+    a.ninst = B->ninst;
+    a.s_istride = ns;
+    a.tg_istride = (size_t)NGA * N * H;
+    a.tx_istride = (size_t)PF_COUNT * N * H;
+    a.p_istride = (size_t)PF_COUNT * N * N;
+    a.a_istride = B->have_alpha ? (size_t)N * N : 0;
+    a.g_istride = (size_t)N * N;
+    std::vector<real> lw(ni, (real)0);   // dL/dloss_k / window per instance
+    bool any_loss = false;
+    if (glosses && B->window > 0)
+        for (size_t k = 0; k < ni; ++k) {
+            lw[k] = (real)(glosses[k] / B->window);
+            any_loss |= glosses[k] != 0.0;
+        }
+    QAF_CUDA(cudaMemcpyAsync(B->lossw, lw.data(), ni * sizeof(real), cudaMemcpyHostToDevice, st));
+    a.loss_wv = reinterpret_cast<const real*>(B->lossw);
+    for (int f = 0; f < 3; ++f) {
+        if (gT[f]) QAF_CUDA(cudaMemcpyAsync(a.sbar[f], gT[f], ni * ns * cb, cudaMemcpyDeviceToDevice, st));
+        else QAF_CUDA(cudaMemsetAsync(a.sbar[f], 0, ni * ns * cb, st));
+    }
+    QAF_CUDA(cudaMemsetAsync(B->agrad, 0, ni * N * N * sizeof(real), st));
+    const int T = B->nsteps;
+    auto in_window = [&](int n) { return B->window > 0 && any_loss && n >= T - B->window + 1; };
+    auto col = [&]() { adj_colp_kernel<real, N, W, EC><<<(H / W + 1) * B->ninst, COL_THREADS, COL_SMEM, st>>>(a); };
+    const size_t slot = ni * PF_COUNT * N * N;
+    bool started = false;
+    for (int seg = B->nseg - 1; seg >= 0; --seg) {
+        const int t0 = seg * B->K, t1 = std::min(T, t0 + B->K);
+        unsigned char* c = B->ckpt + (size_t)seg * 3 * ni * ns * cb;
+        const cplx<real>* src[3] = {bfield<real>(c, ns, B->ninst, 0), bfield<real>(c, ns, B->ninst, 1),
+                                    bfield<real>(c, ns, B->ninst, 2)};
+        QAF_TRY(O::load(B, src, ns, st));
+        // w after local step s (state t0 + s + 1) for the states in the loss window
+        const int wfrom = std::max(0, T - B->window - t0);
+        QAF_TRY(O::template advance<N>(B, t1 - t0, reinterpret_cast<real*>(B->phys), reinterpret_cast<cplx<real>*>(B->wlog),
+                                       wfrom, false, 0, 0.0, st));
+        auto w_at = [&](int n) -> const cplx<real>* {   // w of the state at time n, t0 <= n <= t1
+            if (n == t0) return bfield<real>(c, ns, B->ninst, 0);
+            return reinterpret_cast<const cplx<real>*>(B->wlog) + (size_t)(n - 1 - t0 - wfrom) * ni * ns;
+        };
+        for (int n = t1 - 1; n >= t0; --n) {
+            if (!started) {
+                a.stage = 0; a.emit = 1;
+                a.wstate = in_window(T) ? w_at(T) : nullptr;
+                col();
+                started = true;
+            }
+            for (int s = 4; s >= 1; --s) {
+                a.phys = reinterpret_cast<const real*>(B->phys) + ((size_t)(n - t0) * 4 + (s - 1)) * slot;
+                adj_row_kernel<real, N, ER><<<N * B->ninst, ROW_THREADS, ROW_SMEM, st>>>(a);
+                a.stage = s;
+                a.emit = (s > 1 || n > 0) ? 1 : 0;
+                a.wstate = (s == 1 && in_window(n)) ? w_at(n) : nullptr;
+                col();
+            }
+        }
+    }
+    for (int f = 0; f < 3; ++f)
+        if (g0[f]) QAF_CUDA(cudaMemcpyAsync(g0[f], a.sbar[f], ni * ns * cb, cudaMemcpyDeviceToDevice, st));
+    if (galpha) QAF_CUDA(cudaMemcpyAsync(galpha, B->agrad, ni * N * N * sizeof(real), cudaMemcpyDeviceToDevice, st));
+    return post_launch("qaf_adjoint_batch_backward");
+}
+
+template <class F>
+qaf_status with_small_n(int N, F&& f) {
+    switch (N) {
+        case 16: return f(std::integral_constant<int, 16>{});
+        case 32: return f(std::integral_constant<int, 32>{});
+        case 64: return f(std::integral_constant<int, 64>{});
+        case 128: return f(std::integral_constant<int, 128>{});
+        case 256: return f(std::integral_constant<int, 256>{});
+        default: return fail(QAF_ERR_UNSUPPORTED, "batched adjoint: grids up to 256 x 256");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+qaf_status qaf_adjoint_batch_create(int ninst, int n, double lx, double ly, qaf_dtype dtype, const qaf_params* p,
+                                    int nsteps, int checkpoint_every, int loss_window, qaf_adjoint_batch** out) {
+    if (!out || !p) return fail(QAF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (ninst < 1) return fail(QAF_ERR_INVALID, "ninst must be >= 1");
+    if (n > 256) return fail(QAF_ERR_UNSUPPORTED, "batched adjoint: grids up to 256 x 256");
+    if (nsteps < 1 || checkpoint_every < 1) return fail(QAF_ERR_INVALID, "nsteps and checkpoint_every must be >= 1");
+    if (loss_window < 0 || loss_window > nsteps) return fail(QAF_ERR_INVALID, "loss_window must be in [0, nsteps]");
+    std::vector<int> sizes(ninst, n);
+    std::vector<double> al(ninst, p->alpha), rf(ninst, p->rf);
+    qaf_adjoint_batch* B = new qaf_adjoint_batch();
+    qaf_status s = qaf_ensemble_create(ninst, sizes.data(), lx, ly, dtype, p, al.data(), rf.data(), &B->ens);
+    if (s != QAF_OK) { delete B; return s; }
+    B->ninst = ninst; B->n = n; B->nsteps = nsteps; B->K = std::min(checkpoint_every, nsteps);
+    B->window = loss_window; B->nseg = (nsteps + B->K - 1) / B->K;
+    B->ns = (size_t)(n / 2 + 1) * n; B->np = (size_t)n * n;
+    const size_t rb = dtype == QAF_F64 ? 8 : 4, cb = 2 * rb, ni = (size_t)ninst;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    const size_t o_ck = take((size_t)B->nseg * 3 * ni * B->ns * cb);
+    const size_t o_wl = take((size_t)std::min(B->K, std::max(loss_window, 1)) * ni * B->ns * cb);
+    const size_t o_ph = take((size_t)B->K * 4 * ni * PF_COUNT * B->np * rb);
+    const size_t o_tg = take(ni * NGA * n * (n / 2) * cb);
+    const size_t o_tx = take(ni * PF_COUNT * n * (n / 2) * cb);
+    const size_t o_ab = take(3 * ni * B->ns * cb), o_sa = take(3 * ni * B->ns * cb), o_sb = take(3 * ni * B->ns * cb);
+    const size_t o_ag = take(ni * B->np * rb), o_al = take(ni * B->np * rb), o_lw = take(ni * rb);
+    const size_t o_ls = take(ni * sizeof(double));
+    cudaError_t e = cudaMalloc((void**)&B->blk, off);
+    if (e != cudaSuccess) {
+        qaf_ensemble_destroy(B->ens);
+        delete B;
+        return fail(QAF_ERR_ALLOC, std::string("qaf_adjoint_batch_create: cudaMalloc of ") + std::to_string(off >> 20) +
+                                       " MiB: " + cudaGetErrorString(e));
+    }
+    B->ckpt = B->blk + o_ck; B->wlog = B->blk + o_wl; B->phys = B->blk + o_ph; B->Tg = B->blk + o_tg;
+    B->Tx = B->blk + o_tx; B->abar = B->blk + o_ab; B->sacc = B->blk + o_sa; B->sbar = B->blk + o_sb;
+    B->agrad = B->blk + o_ag; B->alpha = B->blk + o_al; B->lossw = B->blk + o_lw;
+    B->loss = reinterpret_cast<double*>(B->blk + o_ls);
+    *out = B;
+    return QAF_OK;
+}
+
+qaf_status qaf_adjoint_batch_destroy(qaf_adjoint_batch* B) {
+    if (!B) return QAF_OK;
+    if (B->blk) cudaFree(B->blk);
+    qaf_ensemble_destroy(B->ens);
+    delete B;
+    return QAF_OK;
+}
+
+qaf_status qaf_adjoint_batch_forward(qaf_adjoint_batch* B, const void* w0, const void* r1_0, const void* r2_0,
+                                     const void* alpha, void* wT, void* r1T, void* r2T, double* losses, void* stream) {
+    if (!B) return fail(QAF_ERR_INVALID, "null batch");
+    if (!w0 || !r1_0 || !r2_0) return fail(QAF_ERR_INVALID, "null initial state");
+    const void* s0[3] = {w0, r1_0, r2_0};
+    void* sT[3] = {wT, r1T, r2T};
+    B->have_forward = false;
+    QAF_TRY(with_small_n(B->n, [&](auto nn) -> qaf_status {
+        constexpr int N = decltype(nn)::value;
+        return B->ens->dtype == QAF_F64 ? batch_forward<double, N>(B, s0, alpha, sT, losses, (cudaStream_t)stream)
+                                        : batch_forward<float, N>(B, s0, alpha, sT, losses, (cudaStream_t)stream);
+    }));
+    B->have_forward = true;
+    return QAF_OK;
+}
+
+qaf_status qaf_adjoint_batch_backward(qaf_adjoint_batch* B, const void* gwT, const void* gr1T, const void* gr2T,
+                                      const double* glosses, void* gw0, void* gr1_0, void* gr2_0, void* galpha,
+                                      void* stream) {
+    if (!B) return fail(QAF_ERR_INVALID, "null batch");
+    if (!B->have_forward) return fail(QAF_ERR_INVALID, "qaf_adjoint_batch_backward needs a forward first");
+    const void* gT[3] = {gwT, gr1T, gr2T};
+    void* g0[3] = {gw0, gr1_0, gr2_0};
+    return with_small_n(B->n, [&](auto nn) -> qaf_status {
+        constexpr int N = decltype(nn)::value;
+        return B->ens->dtype == QAF_F64 ? batch_backward<double, N>(B, gT, glosses, g0, galpha, (cudaStream_t)stream)
+                                        : batch_backward<float, N>(B, gT, glosses, g0, galpha, (cudaStream_t)stream);
+    });
+}
+
+}  // extern "C"

@@ -638,13 +638,13 @@ struct RowKernel {
     __device__ void zero_slot0(int g) const { if (t == 0) grow(g)[0] = mk<real>(0, 0); }
     __device__ void dump(int fld, const cplx<real> (&v)[E], bool imag) const {
         if (!a.phys_out) return;
-        real* o = a.phys_out + (size_t)fld * N * N + (size_t)n * N;
+        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * N + (size_t)n * N;
 #pragma unroll
         for (int e = 0; e < E; ++e) o[t + TEAM * e] = imag ? v[e].y : v[e].x;
     }
     __device__ void dump_slot(int fld, int slot) const {
         if (!a.phys_out) return;
-        real* o = a.phys_out + (size_t)fld * N * N + (size_t)n * N;
+        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * N + (size_t)n * N;
 #pragma unroll
         for (int e = 0; e < E; ++e) o[t + TEAM * e] = kp(slot, e);
     }
@@ -820,6 +820,32 @@ __global__ void internal_to_ref(const cplx<real>* __restrict__ m, const cplx<rea
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
         const int j = (int)(k / nxh), i = (int)(k % nxh);
         ref[k] = (i < H) ? m[tidx(N, i, j)] : nq[j];
+    }
+}
+
+// batched forms: instance k (blockIdx.y) at m + k * istride, nq + k * istride, ref + k * ref_istride
+template <typename real>
+__global__ void ref_to_internal_batch(const cplx<real>* __restrict__ ref, size_t ref_istride, cplx<real>* __restrict__ m,
+                                      cplx<real>* __restrict__ nq, size_t istride, int N) {
+    const int H = N / 2, nxh = H + 1;
+    const size_t total = (size_t)nxh * N;
+    const size_t k0 = blockIdx.y;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(k / nxh), i = (int)(k % nxh);
+        const cplx<real> v = ref[k0 * ref_istride + k];
+        if (i < H) m[k0 * istride + tidx(N, i, j)] = v;
+        else nq[k0 * istride + j] = v;
+    }
+}
+template <typename real>
+__global__ void internal_to_ref_batch(const cplx<real>* __restrict__ m, const cplx<real>* __restrict__ nq, size_t istride,
+                                      cplx<real>* __restrict__ ref, size_t ref_istride, int N) {
+    const int H = N / 2, nxh = H + 1;
+    const size_t total = (size_t)nxh * N;
+    const size_t k0 = blockIdx.y;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(k / nxh), i = (int)(k % nxh);
+        ref[k0 * ref_istride + k] = (i < H) ? m[k0 * istride + tidx(N, i, j)] : nq[k0 * istride + j];
     }
 }
 

@@ -102,6 +102,7 @@ struct alignas(64) StageArgs {
     int* queue;            // work counter of the persistent column kernel (reset by the row kernel)
     real* phys_out;        // optional: 9 physical fields + S + p11 p12 p21 (13 * N * N)
     int phys_all;          // with phys_out: also S, p11, p12, p21 (else the 9 fields only)
+    size_t phys_istride;   // reals between instances' phys_out blocks
     // batches of independent instances of the same grid: every buffer above
     // (state, intermediates, D, Ed) of instance k sits istride complex elements
     // after instance k-1's; per-instance parameters come from the inst_ arrays

@@ -40,7 +40,8 @@ EXPORTS = [
     "qaf_ensemble_init_random", "qaf_ensemble_load", "qaf_ensemble_store", "qaf_ensemble_advance",
     "qaf_ensemble_diagnostics", "qaf_ensemble_set_controls", "qaf_adjoint_create", "qaf_adjoint_destroy",
     "qaf_adjoint_forward", "qaf_adjoint_backward", "qaf_autotune", "qaf_autotune_load", "qaf_autotune_reset",
-    "qaf_set_variant", "qaf_variant_choice", "qaf_variant_list",
+    "qaf_set_variant", "qaf_variant_choice", "qaf_variant_list", "qaf_adjoint_batch_create",
+    "qaf_adjoint_batch_destroy", "qaf_adjoint_batch_forward", "qaf_adjoint_batch_backward",
 ]
 
 
@@ -150,6 +151,11 @@ def lib():
         L.qaf_set_variant.argtypes = [cp, cp, cp, sp, sp]
         L.qaf_variant_choice.argtypes = [cp, cp, cp, sp, cp]
         L.qaf_variant_list.argtypes = [cp, cp, sp, cp]
+        L.qaf_adjoint_batch_create.argtypes = [cp, cp, ctypes.c_double, ctypes.c_double, cp, ctypes.POINTER(CParams),
+                                               cp, cp, cp, ctypes.POINTER(vp)]
+        L.qaf_adjoint_batch_destroy.argtypes = [vp]
+        L.qaf_adjoint_batch_forward.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, dp, vp]
+        L.qaf_adjoint_batch_backward.argtypes = [vp, vp, vp, vp, dp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -545,5 +551,61 @@ class Adjoint:
         _check(lib().qaf_adjoint_backward(self._h, *g, float(grad_loss), m._chk_spec(gw), m._chk_spec(g1),
                                           m._chk_spec(g2), m._chk_phys(ga) if ga is not None else None,
                                           _stream()))
+        return gw, g1, g2, ga
+
+
+class AdjointBatch:
+    """`ninst` instances of one n x n grid (n <= 256) with their own initial
+    spectra and activity fields, stepped and differentiated together
+    (qaf_adjoint_batch_*): each stage of the forward, recompute and adjoint is
+    one launch for the whole batch. Tensors hold the instances along dim 0."""
+
+    def __init__(self, ninst: int, n: int, p: Params, nsteps: int, checkpoint_every: int = 64, loss_window: int = 1,
+                 lx: float = 2 * math.pi, dtype: int = F32):
+        self.ninst, self.n, self.nsteps, self.dtype = ninst, n, nsteps, dtype
+        self.mesh = Mesh(n, n, lx, lx, dtype)          # tensor shapes and dtypes
+        cp = p.c()
+        h = ctypes.c_void_p()
+        _check(lib().qaf_adjoint_batch_create(ninst, n, lx, lx, dtype, ctypes.byref(cp), nsteps, checkpoint_every,
+                                              loss_window, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.qaf_adjoint_batch_destroy(h)
+            self._h = None
+
+    def _spec(self):
+        import torch
+        return torch.zeros((self.ninst, self.n, self.n // 2 + 1), dtype=self.mesh.complex_dtype, device="cuda")
+
+    def _chk(self, t, real=False):
+        shape = (self.ninst, self.n, self.n) if real else (self.ninst, self.n, self.n // 2 + 1)
+        dt = self.mesh.real_dtype if real else self.mesh.complex_dtype
+        if tuple(t.shape) != shape or t.dtype != dt:
+            raise ValueError(f"expected {shape} {dt}, got {tuple(t.shape)} {t.dtype}")
+        return _ptr(t)
+
+    def forward(self, w0, r1_0, r2_0, alpha=None, final_state: bool = True):
+        """Returns (losses (list of ninst floats), (wT, r1T, r2T) or None)."""
+        out = (self._spec(), self._spec(), self._spec()) if final_state else None
+        ptrs = [self._chk(t) for t in out] if out else [None, None, None]
+        losses = (ctypes.c_double * self.ninst)()
+        _check(lib().qaf_adjoint_batch_forward(self._h, self._chk(w0), self._chk(r1_0), self._chk(r2_0),
+                                               self._chk(alpha, True) if alpha is not None else None, *ptrs, losses,
+                                               _stream()))
+        return list(losses), out
+
+    def backward(self, grad_final=None, grad_losses=None, want_alpha: bool = True):
+        """(gw0, gr1_0, gr2_0, galpha) for dL/d(final states) (or None) and dL/dloss_k (or None)."""
+        import torch
+        keep = [t.contiguous() if t is not None else None for t in grad_final] if grad_final is not None else []
+        g = [self._chk(t) if t is not None else None for t in keep] if keep else [None, None, None]
+        gl = (ctypes.c_double * self.ninst)(*[float(v) for v in grad_losses]) if grad_losses is not None else None
+        gw, g1, g2 = self._spec(), self._spec(), self._spec()
+        ga = torch.zeros((self.ninst, self.n, self.n), dtype=self.mesh.real_dtype, device="cuda") if want_alpha else None
+        _check(lib().qaf_adjoint_batch_backward(self._h, *g, gl, self._chk(gw), self._chk(g1), self._chk(g2),
+                                                self._chk(ga, True) if ga is not None else None, _stream()))
         return gw, g1, g2, ga
 
