@@ -91,6 +91,7 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
     ap.add_argument("--workload", choices=["plain", "ensemble", "adjoint", "control"], default="plain")
     ap.add_argument("--horizon", type=int, default=CTL_STEPS, help="control workload: steps per rollout")
+    ap.add_argument("--adj-steps", type=int, default=ADJ_STEPS, help="adjoint workload: steps per rollout")
     ap.add_argument("--no-fd", action="store_true", help="adjoint workload: skip the finite-difference check")
     ap.add_argument("--no-tune", action="store_true", help="ensemble workload: keep the built-in launch shapes")
     ap.add_argument("--instances", type=int, default=ENS_COUNT)
@@ -539,7 +540,8 @@ def run_adjoint(a, world, rank, local):
     import qaf
     import qaf.autograd as QA
 
-    n, T, K, Wn, dt = ADJ_N, ADJ_STEPS, ADJ_K, ADJ_WINDOW, ADJ_DT
+    n, T, dt = ADJ_N, a.adj_steps, ADJ_DT
+    K, Wn = min(ADJ_K, T), min(ADJ_WINDOW, T)
     reps, warm = max(1, min(a.steps, 5)), 3
     alpha_np = smoothed_alpha(n, ADJ_SEED)
     base = dict(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=dt, q_lin=1.0, advect_omega=1)

@@ -2285,9 +2285,11 @@ qaf_status batch_backward(qaf_adjoint_batch* B, const void* const* gT, const dou
                           void* galpha, cudaStream_t st) {
     using O = BatchOps<real>;
     constexpr int H = N / 2;
-    constexpr int W = 1, EC = N / 16 > 4 ? N / 16 : 4;
+    // several columns per CTA: coalesced 16-32 byte segments of the T arrays (a batch has CTAs to spare)
+    constexpr int W0 = sizeof(real) == 4 ? 4 : 2;
+    constexpr int W = W0 < H ? W0 : H, EC = N / 16 > 4 ? N / 16 : 4;
     constexpr int COL_THREADS = NGA * W * (N / EC);
-    constexpr size_t COL_SMEM = (size_t)NGA * N * 2 * sizeof(cplx<real>);
+    constexpr size_t COL_SMEM = (size_t)NGA * N * (W > 1 ? W : 2) * sizeof(cplx<real>);
     constexpr int ER = H / 16 < 2 ? 2 : (H / 16 > 16 ? 16 : H / 16);
     constexpr int ROW_THREADS = NGA * (H / ER);
     constexpr size_t ROW_SMEM = (size_t)NGA * H * sizeof(cplx<real>);

@@ -104,6 +104,18 @@ QAF_HD int stockham_dest(int t, int slot) {
     return (b / S) * S * R + (b % S) + r * S;
 }
 
+// ---------------------------------------------------------------------------
+// Exchange-buffer swizzle. A Stockham pass writes its E outputs at stride E
+// (first pass) or in groups of S spaced S*R apart, so 8-byte stores of a
+// half-warp would pile onto a few banks (up to 16-way); reads are contiguous.
+// XOR-ing the element index within each 16-element (128-byte) line with
+// (line * 5) mod 16 spreads every write pattern of the team FFTs over the
+// banks (worst case 2-way; contiguous reads stay a permutation of one line).
+// A bijection of each aligned 16-element line, so buffers whose length is a
+// multiple of 16 (or below 16, where it is the identity) stay in bounds.
+// ---------------------------------------------------------------------------
+QAF_HD int swz(int a) { return a ^ (((a >> 4) * 5) & 15); }
+
 // Radix schedule for L = 2^m with E = 2^e values per thread: as many radix-E
 // passes as fit, then one smaller pass for the remainder.
 template <int L, int E>

@@ -365,7 +365,7 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int in
                     for (int e = 0; e < E; ++e) {
                         const int j = t + TEAM * e;
                         cplx<real> acc = ctab[col * N + j];
-                        for (int ww = 0; ww < W; ++ww) acc = cadd(acc, buf[j * W + ww]);
+                        for (int ww = 0; ww < W; ++ww) acc = cadd(acc, x.read_team(j, ww));
                         ctab[col * N + j] = acc;
                     }
                 x.sync();
@@ -542,8 +542,8 @@ template <typename real, int TEAM, bool NAMED>
 struct XchgTeam {
     cplx<real>* buf;
     int id;
-    __device__ void write(int idx, cplx<real> v) { buf[idx] = v; }
-    __device__ cplx<real> read(int idx) const { return buf[idx]; }
+    __device__ void write(int idx, cplx<real> v) { buf[swz(idx)] = v; }
+    __device__ cplx<real> read(int idx) const { return buf[swz(idx)]; }
     __device__ void sync() {
         if constexpr (NAMED) asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(TEAM) : "memory");
         else __syncthreads();

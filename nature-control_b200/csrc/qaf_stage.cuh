@@ -119,7 +119,8 @@ QAF_HD real ky_of(int j, int N, real dky) { return dky * (real)(j <= N / 2 ? j :
 
 // ---------------------------------------------------------------------------
 // shared-memory exchange for W interleaved teams: element idx of team w at
-// buf[idx * W + w]
+// buf[idx * W + w] (measured: the exchange swizzle of qaf_fft.cuh slows the
+// column kernels, whose interleaved teams already spread the writes)
 // ---------------------------------------------------------------------------
 template <typename real>
 struct XchgCols {
@@ -127,15 +128,16 @@ struct XchgCols {
     int w, W;
     __device__ void write(int idx, cplx<real> v) { buf[idx * W + w] = v; }
     __device__ cplx<real> read(int idx) const { return buf[idx * W + w]; }
+    __device__ cplx<real> read_team(int idx, int team) const { return buf[idx * W + team]; }
     __device__ void sync() { __syncthreads(); }
 };
 
-// one team per row; team r owns buf[r * L ...]
+// one team per row; team r owns buf[r * L ...], element idx at swz(idx)
 template <typename real>
 struct XchgRow {
     cplx<real>* buf;
-    __device__ void write(int idx, cplx<real> v) { buf[idx] = v; }
-    __device__ cplx<real> read(int idx) const { return buf[idx]; }
+    __device__ void write(int idx, cplx<real> v) { buf[swz(idx)] = v; }
+    __device__ cplx<real> read(int idx) const { return buf[swz(idx)]; }
     __device__ void sync() { __syncthreads(); }
 };
 

@@ -24,12 +24,12 @@ void emulate_pass(std::vector<cplx<real>>& regs, const cplx<real>* tw) {
         for (int t = 0; t < TEAM; ++t)
             for (int slot = 0; slot < E; ++slot) {
                 int d = stockham_dest<L, E, R, S>(t, slot);
-                buf[d] = regs[t * E + slot];
+                buf[swz(d)] = regs[t * E + slot];   // through the kernels' exchange swizzle
                 hit[d]++;
             }
         for (int i = 0; i < L; ++i) if (hit[i] != 1) { std::printf("dest map not a permutation\n"); std::exit(1); }
         for (int t = 0; t < TEAM; ++t)
-            for (int e = 0; e < E; ++e) regs[t * E + e] = buf[t + TEAM * e];
+            for (int e = 0; e < E; ++e) regs[t * E + e] = buf[swz(t + TEAM * e)];
         emulate_pass<real, L, E, INV, TWN, P + 1>(regs, tw);
     }
 }
@@ -73,6 +73,14 @@ double check() {
 
 int main() {
     int bad = 0;
+    // the exchange swizzle permutes every buffer length the kernels use (8 .. 8192 elements)
+    for (int len = 8; len <= 8192; len *= 2) {
+        std::vector<int> seen(len, 0);
+        for (int a = 0; a < len; ++a) {
+            const int p = swz(a);
+            if (p < 0 || p >= len || seen[p]++) { std::printf("swizzle not a permutation of [0,%d)\n", len); bad++; break; }
+        }
+    }
     CASE(double, 8, 8, false, 1e-14);  CASE(double, 16, 8, true, 1e-14);
     CASE(double, 32, 8, false, 1e-14); CASE(double, 64, 8, true, 1e-14);
     CASE(double, 128, 4, false, 1e-14); CASE(double, 256, 16, true, 1e-14);

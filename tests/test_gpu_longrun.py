@@ -1,0 +1,40 @@
+"""Long runs: the FP32 path's mean enstrophy, mean energy and time-averaged
+energy spectrum stay within 1% of the FP64 path's (the FP64 path matches the
+reference's own build to 1e-10 over 1000 steps, test_gpu_parity.py). Past a
+few thousand steps pointwise agreement is not expected; statistics are."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(qaf, dtype, n, steps, chunk, nshells):
+    m = qaf.Mesh(n, lx=16 * math.pi, dtype=dtype)
+    p = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=1e-3)
+    m.load(*m.random_q(1))
+    diags, specs = [], []
+    for c in range(steps // chunk):
+        m.advance(p, chunk)
+        diags.append(m.last_diagnostics())
+        if c >= (steps // chunk) // 2:
+            w, _, _ = m.store()
+            specs.append(m.diagnostics(w, nshells=nshells)[2])
+    return np.array(diags), np.mean(specs, axis=0)
+
+
+def test_fp32_statistics_within_one_percent_of_fp64(cuda):
+    import qaf
+    n, steps, chunk, nshells = 128, 16000, 500, 40
+    d32, s32 = _run(qaf, qaf.F32, n, steps, chunk, nshells)
+    d64, s64 = _run(qaf, qaf.F64, n, steps, chunk, nshells)
+    h = len(d64) // 2
+    e32, z32 = d32[h:, 0].mean(), d32[h:, 1].mean()
+    e64, z64 = d64[h:, 0].mean(), d64[h:, 1].mean()
+    assert z64 > 0 and e64 > 0
+    assert abs(z32 - z64) <= 0.01 * z64, (z32, z64)
+    assert abs(e32 - e64) <= 0.01 * e64, (e32, e64)
+    big = s64 > 1e-3 * s64.max()          # the shells that carry the energy
+    rel = np.abs(s32[big] - s64[big]) / s64[big]
+    assert rel.max() <= 0.01, rel.max()
