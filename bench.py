@@ -264,12 +264,12 @@ def run_qaf(a, world, rank, local):
     peak, peak_kind = peaks()
     achieved = k_bytes / (k_ms * 1e-3) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "traffic.txt")   # per-launch DRAM bytes from ncu captures
     if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get(f"{dom}_{a.dtype}_{n}")
-        except Exception:
-            traffic = None
+        for line in open(tpath):
+            f = line.split()
+            if len(f) == 2 and not line.startswith("#") and f[0] == f"{dom}_{a.dtype}_{n}":
+                traffic = float(f[1])
 
     # ---- end to end through the public API, host I/O every step ----------
     alpha_host = torch.ones((n, n), dtype=mesh.real_dtype).pin_memory()
