@@ -93,7 +93,8 @@ def parse():
     ap.add_argument("--horizon", type=int, default=CTL_STEPS, help="control workload: steps per rollout")
     ap.add_argument("--adj-steps", type=int, default=ADJ_STEPS, help="adjoint workload: steps per rollout")
     ap.add_argument("--no-fd", action="store_true", help="adjoint workload: skip the finite-difference check")
-    ap.add_argument("--no-tune", action="store_true", help="ensemble workload: keep the built-in launch shapes")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="ensemble, adjoint and control workloads: keep the built-in launch shapes")
     ap.add_argument("--instances", type=int, default=ENS_COUNT)
     return ap.parse_args()
 
@@ -552,6 +553,9 @@ def run_adjoint(a, world, rank, local):
         p.alpha_field = torch.as_tensor(alpha_np).to(device="cuda", dtype=mesh.real_dtype)
         return mesh, p, mesh.random_q(SEED)
 
+    shapes = "col:default row:default"
+    if not a.no_tune:                         # launch shapes for this grid (untimed)
+        shapes, _ = qaf.autotune(n, qaf.F32, 1, None)
     mesh, p, s0 = setup(qaf.F32)
     adj = qaf.Adjoint(mesh, T, K, Wn)
     ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -630,7 +634,7 @@ def run_adjoint(a, world, rank, local):
         "config": {"workload": f"adjoint {n}x{n} FP32, {T} IF-RK4 steps dt={dt}, Ra(x) = 1 + 0.1 smoothed N(0,1) "
                                f"(width 4 cells, seed {ADJ_SEED}), loss = mean enstrophy of the last {Wn} states, "
                                f"checkpoints every {K} steps", "grid": n, "horizon": T,
-                   "parallelism": f"replicas x{world}",
+                   "launch_shapes": shapes, "parallelism": f"replicas x{world}",
                    "l2": "working set of a segment's recording (~600 MB) larger than L2"},
         "forward_ms": tp, "adjoint_forward_ms": taf, "backward_ms": tbw,
         "ratio_forward_with_checkpoints_plus_backward": (taf + tbw) / tp,
@@ -723,6 +727,9 @@ def run_control(a, world, rank, local):
     n, ni, T, K, lr = CTL_N, CTL_INST, a.horizon, min(CTL_K, a.horizon), CTL_LR
     iters, warm = max(1, min(a.steps, 5)), 1
     p = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=ADJ_DT, q_lin=1.0, advect_omega=1)
+    shapes = {"batched": "col:default row:default", "single": "col:default row:default"}
+    if not a.no_tune:                         # launch shapes for the batch and the looped single grid (untimed)
+        shapes = {"batched": qaf.autotune(n, qaf.F32, ni, None)[0], "single": qaf.autotune(n, qaf.F32, 1, None)[0]}
     batch = qaf.AdjointBatch(ni, n, p, T, K, 1, lx=L, dtype=qaf.F32)
     mesh = batch.mesh
     alpha = torch.stack([torch.as_tensor(smoothed_alpha(n, 100 + k), dtype=torch.float32) for k in range(ni)]).cuda()
@@ -782,7 +789,8 @@ def run_control(a, world, rank, local):
         "config": {"workload": f"control loop: {ni} x {n}^2 FP32, horizon {T} IF-RK4 steps dt={ADJ_DT}, Ra_k(x) = "
                                f"1 + 0.1 smoothed N(0,1) (seeds 100..{100 + ni - 1}), loss = terminal enstrophy, "
                                f"checkpoints every {K} steps, normalised descent step {lr}",
-                   "instances": ni, "grid": n, "horizon": T, "parallelism": f"replicas x{world}",
+                   "instances": ni, "grid": n, "horizon": T, "launch_shapes": shapes,
+                   "parallelism": f"replicas x{world}",
                    "l2": f"recording of a segment ({ni * K * 4 * 9 * pr / 1e9:.0f} GB) larger than L2"},
         "loss_mean_first": l0, "loss_mean_last": lN, "loss_history_mean": [float(np.mean(h)) for h in history],
         "looped": {"value": looped, "unit": "instance-iterations/s", "ms_per_instance_iteration": ms_single,
