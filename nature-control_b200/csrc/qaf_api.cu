@@ -1707,8 +1707,11 @@ struct OpAdjBackward {
         // column pass: field-parallel (11 transform teams per column, one column per CTA) up to 256^2,
         // W columns per CTA with the transforms in sequence above
         constexpr bool FP = N <= 256;
-        constexpr int W = FP ? 1 : C::W;
-        constexpr int EC = FP ? (N / 16 > 4 ? N / 16 : 4) : C::EC;
+        // FP32 from 128^2: 2 columns per CTA with 8-value teams (704 threads, 16-byte segments of the
+        // T arrays); otherwise one column per CTA with 16-value teams (FP64 keeps its registers)
+        constexpr bool W2 = FP && sizeof(real) == 4 && N >= 128;
+        constexpr int W = FP ? (W2 ? 2 : 1) : C::W;
+        constexpr int EC = FP ? (W2 ? N / 32 : (N / 16 > 4 ? N / 16 : 4)) : C::EC;
         constexpr int COL_THREADS = FP ? NGA * W * (N / EC) : W * (N / EC);
         constexpr size_t COL_SMEM = FP ? (size_t)NGA * N * (W > 1 ? W : 2) * sizeof(cplx<real>)
                                        : (size_t)W * N * sizeof(cplx<real>);
