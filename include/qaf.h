@@ -139,6 +139,11 @@ qaf_status qaf_step_host(qaf_mesh* mesh, const qaf_params* p, qaf_integrator int
  * (Lx Ly) (post_process/postprocess.cu:54-65,158-161), out[1] = enstrophy
  * 0.5 <w^2>. Returns QAF_ERR_NONFINITE if a step produced Inf/NaN. */
 qaf_status qaf_last_diagnostics(qaf_mesh* mesh, double out[2]);
+/* The same two values without synchronising: enqueued on `stream` (after the
+ * steps it follows), written to `out` (2 doubles, pinned host or device
+ * memory) when the stream reaches it. No counterpart in the reference. The
+ * non-finite status is left to qaf_last_diagnostics / qaf_check_finite. */
+qaf_status qaf_last_diagnostics_async(qaf_mesh* mesh, double* out, void* stream);
 /* Synchronises `stream` and reports whether any step since the last call
  * produced a non-finite value (the reference's NaN check, friction.cu:280). */
 qaf_status qaf_check_finite(qaf_mesh* mesh, void* stream);

@@ -228,7 +228,8 @@ qaf_status ensure_ws(qaf_mesh* m) {
     size_t oT = take(plane), otw = take(N);
     // real tables stored in complex slots
     size_t oex = take((4 * (H + 1) + 1) / 2 + 1), oey = take((4 * N + 1) / 2 + 1);
-    size_t odiag = take((4 + 512 + 513) * sizeof(double) / sizeof(cplx<real>) + 1);
+    // [0, 2) step sums, [2, 4) diagnostics, [4, 516) spectrum, [516, 1029) shell bounds, [1029, 1031) async copy-out
+    size_t odiag = take((4 + 512 + 513 + 2) * sizeof(double) / sizeof(cplx<real>) + 1);
     size_t oflags = take(1);
     size_t oqueue = take(1);
     cplx<real>* b = nullptr;
@@ -910,6 +911,20 @@ qaf_status qaf_last_diagnostics(qaf_mesh* m, double out[2]) {
     out[1] = 0.5 * h[0] / n4;   // enstrophy: sum |w|^2
     if (flags & FLAG_WAIT_TIMEOUT) return fail(QAF_ERR_CUDA, "a kernel's wait for its own copy timed out");
     if (flags) return fail(QAF_ERR_NONFINITE, "a step produced a non-finite value");
+    return QAF_OK;
+}
+
+qaf_status qaf_last_diagnostics_async(qaf_mesh* m, double* out, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!out) return fail(QAF_ERR_INVALID, "null pointer");
+    double* diag = m->desc.dtype == QAF_F64 ? m->wd.diag : m->wf.diag;
+    if (!diag) return fail(QAF_ERR_INVALID, "no step has run on this mesh");
+    cudaStream_t st = (cudaStream_t)stream;
+    const double n4 = (double)m->desc.nx * m->desc.ny * (double)m->desc.nx * m->desc.ny;
+    double* staged = diag + 4 + 512 + 513;
+    diag_finalize_kernel<<<1, 32, 0, st>>>(diag, staged, n4);
+    QAF_TRY(post_launch("qaf_last_diagnostics_async"));
+    QAF_CUDA(cudaMemcpyAsync(out, staged, 2 * sizeof(double), cudaMemcpyDefault, st));
     return QAF_OK;
 }
 

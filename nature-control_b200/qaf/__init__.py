@@ -35,7 +35,7 @@ EXPORTS = [
     "qaf_field_alloc", "qaf_field_free", "qaf_mesh_tables", "qaf_fwd_trans", "qaf_bwd_trans", "qaf_symmetrize",
     "qaf_xderiv", "qaf_yderiv", "qaf_laplacian", "qaf_vel", "qaf_dealias", "qaf_if_tables", "qaf_integrate",
     "qaf_nonlinear", "qaf_step", "qaf_step_host", "qaf_last_diagnostics", "qaf_check_finite", "qaf_diagnostics",
-    "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_state_advance_timed", "qaf_launch_count",
+    "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_last_diagnostics_async", "qaf_state_advance_timed", "qaf_launch_count",
     "qaf_init_random_q", "qaf_step_noalloc", "qaf_ensemble_create", "qaf_ensemble_destroy",
     "qaf_ensemble_init_random", "qaf_ensemble_load", "qaf_ensemble_store", "qaf_ensemble_advance",
     "qaf_ensemble_diagnostics", "qaf_ensemble_set_controls", "qaf_adjoint_create", "qaf_adjoint_destroy",
@@ -117,6 +117,7 @@ def lib():
         L.qaf_step.argtypes = [vp, ctypes.POINTER(CParams), cp, vp, vp, vp, cp, vp]
         L.qaf_step_host.argtypes = [vp, ctypes.POINTER(CParams), cp, vp, vp, vp, cp]
         L.qaf_last_diagnostics.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.qaf_last_diagnostics_async.argtypes = [vp, vp, vp]
         L.qaf_check_finite.argtypes = [vp, vp]
         L.qaf_diagnostics.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double), cp, vp]
@@ -398,6 +399,20 @@ class Mesh:
         out = (ctypes.c_double * 2)()
         _check(lib().qaf_last_diagnostics(self._h, out))
         return out[0], out[1]
+
+    def last_diagnostics_async(self, out=None):
+        """Enqueue a read-back of (energy, enstrophy) of the last step into `out`
+        (a float64 tensor of 2, pinned host memory or on the device; a new pinned
+        one if None) without synchronising; valid once the stream reaches it."""
+        import torch
+        if out is None:
+            out = torch.empty(2, dtype=torch.float64).pin_memory()
+        if out.dtype != torch.float64 or out.numel() < 2 or not out.is_contiguous():
+            raise ValueError("out must be a contiguous float64 tensor of 2")
+        if not out.is_cuda and not out.is_pinned():
+            raise ValueError("out must be pinned host memory or a device tensor")
+        _check(lib().qaf_last_diagnostics_async(self._h, ctypes.c_void_p(out.data_ptr()), _stream()))
+        return out
 
     def check_finite(self):
         _check(lib().qaf_check_finite(self._h, _stream()))

@@ -340,3 +340,28 @@ def test_invalid_arguments_are_rejected(cuda):
     with pytest.raises(qaf.QafError) as e:
         m48.step(qaf.Params(), *s48)
     assert e.value.status == qaf.ERR_UNSUPPORTED
+
+
+def test_last_diagnostics_async_equals_sync(cuda):
+    """The asynchronous read-back of (energy, enstrophy) gives what qaf_last_diagnostics gives."""
+    import torch
+
+    import qaf
+    m = qaf.Mesh(64, lx=16 * np.pi, dtype=qaf.F64)
+    m.load(*m.random_q(3))
+    p = qaf.Params(dt=1e-3)
+    host = torch.zeros((3, 2), dtype=torch.float64).pin_memory()
+    dev = torch.zeros(2, dtype=torch.float64, device="cuda")
+    sync = []
+    for k in range(3):
+        m.advance(p, 2)
+        m.last_diagnostics_async(host[k])
+        sync.append(m.last_diagnostics())
+    m.last_diagnostics_async(dev)
+    torch.cuda.synchronize()
+    for k in range(3):
+        assert host[k, 0].item() == sync[k][0] and host[k, 1].item() == sync[k][1]
+    assert dev[0].item() == sync[-1][0]
+    with pytest.raises(ValueError):
+        m.last_diagnostics_async(torch.zeros(2, dtype=torch.float64))   # pageable host memory
+
