@@ -156,6 +156,13 @@ qaf_status qaf_check_finite(qaf_mesh* mesh, void* stream);
 qaf_status qaf_state_load(qaf_mesh* mesh, const void* w, const void* r1, const void* r2, void* stream);
 qaf_status qaf_state_advance(qaf_mesh* mesh, const qaf_params* p, qaf_integrator integ, int nsteps, void* stream);
 qaf_status qaf_state_store(qaf_mesh* mesh, void* w, void* r1, void* r2, void* stream);
+/* Exact checkpoint/restart of the resident state (replaces the reference's
+ * CSV dumps, friction.cu:262-278, BasicUtils.cuh:38-50, which round the
+ * state): a binary file with the grid, precision, domain, a step counter and
+ * the three spectra in the reference layout, bit for bit. restore checks that
+ * the file matches the mesh and loads the state (as qaf_state_load). */
+qaf_status qaf_state_save(qaf_mesh* mesh, const char* path, uint64_t step, void* stream);
+qaf_status qaf_state_restore(qaf_mesh* mesh, const char* path, uint64_t* step, void* stream);
 /* Advance the resident state by nsteps steps with CUDA events recorded on
  * `stream` around every row and column kernel; out_ms[0] / out_ms[1] = mean
  * duration of one row / one column kernel, out_ms[2] = their launch count.

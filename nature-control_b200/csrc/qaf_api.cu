@@ -914,6 +914,74 @@ qaf_status qaf_last_diagnostics(qaf_mesh* m, double out[2]) {
     return QAF_OK;
 }
 
+// Checkpoint file: "QAFSTAT1", int32 nx, ny, dtype (0 f32, 1 f64), pad, double lx, ly,
+// uint64 step, then the w, r1, r2 spectra in the reference layout (i + j*(nx/2+1)),
+// interleaved (re, im), little-endian as the host writes them.
+qaf_status qaf_state_save(qaf_mesh* m, const char* path, uint64_t step, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!path) return fail(QAF_ERR_INVALID, "null path");
+    if (!m->loaded) return fail(QAF_ERR_INVALID, "no state loaded on this mesh");
+    const size_t nb = spec_elems(m) * 2 * real_bytes(m);
+    void* d = nullptr;
+    QAF_CUDA(cudaMalloc(&d, 3 * nb));
+    char* dc = static_cast<char*>(d);
+    std::vector<char> h(3 * nb);
+    qaf_status s = qaf_state_store(m, dc, dc + nb, dc + 2 * nb, stream);
+    cudaError_t e = cudaSuccess;
+    if (s == QAF_OK) e = cudaMemcpyAsync(h.data(), d, 3 * nb, cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    cudaFree(d);
+    if (s != QAF_OK) return s;
+    if (e != cudaSuccess) return fail(QAF_ERR_CUDA, std::string("qaf_state_save: ") + cudaGetErrorString(e));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(QAF_ERR_INVALID, std::string("cannot write ") + path);
+    const int32_t hdr[4] = {m->desc.nx, m->desc.ny, m->desc.dtype == QAF_F64 ? 1 : 0, 0};
+    const double geo2[2] = {m->desc.lx, m->desc.ly};
+    bool ok = std::fwrite("QAFSTAT1", 1, 8, f) == 8 && std::fwrite(hdr, sizeof(hdr), 1, f) == 1 &&
+              std::fwrite(geo2, sizeof(geo2), 1, f) == 1 && std::fwrite(&step, sizeof(step), 1, f) == 1 &&
+              std::fwrite(h.data(), 1, h.size(), f) == h.size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? QAF_OK : fail(QAF_ERR_INVALID, std::string("short write to ") + path);
+}
+
+qaf_status qaf_state_restore(qaf_mesh* m, const char* path, uint64_t* step, void* stream) {
+    QAF_TRY(check_mesh(m));
+    if (!path) return fail(QAF_ERR_INVALID, "null path");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(QAF_ERR_INVALID, std::string("cannot read ") + path);
+    char magic[8];
+    int32_t hdr[4];
+    double geo2[2];
+    uint64_t st = 0;
+    const size_t nb = spec_elems(m) * 2 * real_bytes(m);
+    std::vector<char> h(3 * nb);
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "QAFSTAT1", 8) == 0 &&
+              std::fread(hdr, sizeof(hdr), 1, f) == 1 && std::fread(geo2, sizeof(geo2), 1, f) == 1 &&
+              std::fread(&st, sizeof(st), 1, f) == 1;
+    if (!ok) { std::fclose(f); return fail(QAF_ERR_INVALID, std::string(path) + ": not a qaf state file"); }
+    if (hdr[0] != m->desc.nx || hdr[1] != m->desc.ny || hdr[2] != (m->desc.dtype == QAF_F64 ? 1 : 0) ||
+        geo2[0] != m->desc.lx || geo2[1] != m->desc.ly) {
+        std::fclose(f);
+        return fail(QAF_ERR_INVALID, std::string(path) + ": grid, precision or domain differ from the mesh");
+    }
+    ok = std::fread(h.data(), 1, h.size(), f) == h.size();
+    std::fclose(f);
+    if (!ok) return fail(QAF_ERR_INVALID, std::string(path) + ": truncated");
+    void* d = nullptr;
+    QAF_CUDA(cudaMalloc(&d, 3 * nb));
+    char* dc = static_cast<char*>(d);
+    cudaError_t e = cudaMemcpyAsync(d, h.data(), 3 * nb, cudaMemcpyHostToDevice, (cudaStream_t)stream);
+    qaf_status s = e == cudaSuccess ? qaf_state_load(m, dc, dc + nb, dc + 2 * nb, stream)
+                                    : fail(QAF_ERR_CUDA, cudaGetErrorString(e));
+    if (s == QAF_OK) {
+        e = cudaStreamSynchronize((cudaStream_t)stream);   // h and d go out of scope
+        if (e != cudaSuccess) s = fail(QAF_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaFree(d);
+    if (s == QAF_OK && step) *step = st;
+    return s;
+}
+
 qaf_status qaf_last_diagnostics_async(qaf_mesh* m, double* out, void* stream) {
     QAF_TRY(check_mesh(m));
     if (!out) return fail(QAF_ERR_INVALID, "null pointer");

@@ -35,7 +35,7 @@ EXPORTS = [
     "qaf_field_alloc", "qaf_field_free", "qaf_mesh_tables", "qaf_fwd_trans", "qaf_bwd_trans", "qaf_symmetrize",
     "qaf_xderiv", "qaf_yderiv", "qaf_laplacian", "qaf_vel", "qaf_dealias", "qaf_if_tables", "qaf_integrate",
     "qaf_nonlinear", "qaf_step", "qaf_step_host", "qaf_last_diagnostics", "qaf_check_finite", "qaf_diagnostics",
-    "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_last_diagnostics_async", "qaf_state_advance_timed", "qaf_launch_count",
+    "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_last_diagnostics_async", "qaf_state_save", "qaf_state_restore", "qaf_state_advance_timed", "qaf_launch_count",
     "qaf_init_random_q", "qaf_step_noalloc", "qaf_ensemble_create", "qaf_ensemble_destroy",
     "qaf_ensemble_init_random", "qaf_ensemble_load", "qaf_ensemble_store", "qaf_ensemble_advance",
     "qaf_ensemble_diagnostics", "qaf_ensemble_set_controls", "qaf_adjoint_create", "qaf_adjoint_destroy",
@@ -118,6 +118,8 @@ def lib():
         L.qaf_step_host.argtypes = [vp, ctypes.POINTER(CParams), cp, vp, vp, vp, cp]
         L.qaf_last_diagnostics.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.qaf_last_diagnostics_async.argtypes = [vp, vp, vp]
+        L.qaf_state_save.argtypes = [vp, ctypes.c_char_p, ctypes.c_uint64, vp]
+        L.qaf_state_restore.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64), vp]
         L.qaf_check_finite.argtypes = [vp, vp]
         L.qaf_diagnostics.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double), cp, vp]
@@ -379,6 +381,16 @@ class Mesh:
         r2 = self.new_spec() if r2 is None else r2
         _check(lib().qaf_state_store(self._h, self._chk_spec(w), self._chk_spec(r1), self._chk_spec(r2), _stream()))
         return w, r1, r2
+
+    def save(self, path: str, step: int = 0):
+        """Write the resident state to a checkpoint file (exact, with a step counter)."""
+        _check(lib().qaf_state_save(self._h, str(path).encode(), int(step), _stream()))
+
+    def restore(self, path: str) -> int:
+        """Load the resident state from a checkpoint file; returns its step counter."""
+        st = ctypes.c_uint64()
+        _check(lib().qaf_state_restore(self._h, str(path).encode(), ctypes.byref(st), _stream()))
+        return st.value
 
     def advance(self, p: Params, nsteps: int = 1, integrator: int = IFRK4):
         cp = p.c()

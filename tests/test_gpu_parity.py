@@ -365,3 +365,34 @@ def test_last_diagnostics_async_equals_sync(cuda):
     with pytest.raises(ValueError):
         m.last_diagnostics_async(torch.zeros(2, dtype=torch.float64))   # pageable host memory
 
+
+@pytest.mark.parametrize("dtype_name", ["F64", "F32"])
+def test_checkpoint_restart_is_exact(cuda, tmp_path, dtype_name):
+    """10 steps in one go equal 4 steps, a checkpoint file, a fresh mesh restored from it and 6 more steps."""
+    import torch
+
+    import qaf
+    dt = getattr(qaf, dtype_name)
+    p = qaf.Params(dt=1e-3)
+    a = qaf.Mesh(64, lx=16 * np.pi, dtype=dt)
+    s0 = a.random_q(9)
+    a.load(*s0)
+    a.advance(p, 10)
+    want = a.store()
+    b = qaf.Mesh(64, lx=16 * np.pi, dtype=dt)
+    b.load(*s0)
+    b.advance(p, 4)
+    path = tmp_path / "state.qaf"
+    b.save(path, step=4)
+    c = qaf.Mesh(64, lx=16 * np.pi, dtype=dt)
+    assert c.restore(path) == 4
+    c.advance(p, 6)
+    for x, y in zip(c.store(), want):
+        assert torch.equal(x, y)
+    other = qaf.Mesh(32, lx=16 * np.pi, dtype=dt)
+    with pytest.raises(qaf.QafError):
+        other.restore(path)                     # grid differs
+    (tmp_path / "bad.qaf").write_bytes(b"not a state")
+    with pytest.raises(qaf.QafError):
+        c.restore(tmp_path / "bad.qaf")
+
