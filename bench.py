@@ -212,12 +212,31 @@ def cpu_baseline(n, steps, dtype_name):
     s0 = O.initial_spectra(SEED, n)
     O.step(p, *s0, 1)          # warm the FFT plans
     t0 = time.perf_counter()
-    O.step(p, *s0, steps)
+    final = O.step(p, *s0, steps)
     dt = time.perf_counter() - t0
     cores = int(os.environ.get("QAF_ORACLE_THREADS", os.cpu_count() or 1))
-    return {"value": n * n * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+    line = {"value": n * n * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{steps} IF-RK4 steps of the {n}^2 workload in FP64 ({dt:.1f} s) with the host oracle, "
                       f"which follows the reference's operation sequence (~120 2D FFTs per step)"}
+    return line, (O, p, final)
+
+
+def spectrum_vs_oracle(mesh, qaf, oracle_run, steps, nshells=64):
+    """Energy spectrum, energy and enstrophy of the GPU state after `steps` steps of the
+    workload against the oracle's (the state the CPU-baseline leg computed)."""
+    import numpy as np
+    O, p, final = oracle_run
+    pq = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=DT, q_lin=1.0, advect_omega=1)
+    mesh.load(*mesh.random_q(SEED))
+    mesh.advance(pq, steps)
+    w, _, _ = mesh.store()
+    e, z, spec = mesh.diagnostics(w, nshells)
+    eo, zo, speco = O.diagnostics(p, final[0], nshells)
+    big = speco > 1e-6 * speco.max()
+    return {"steps": steps, "shells": nshells,
+            "max_rel_err_shells": float(np.max(np.abs(spec[big] - speco[big]) / speco[big])),
+            "energy_rel_err": abs(e - eo) / abs(eo), "enstrophy_rel_err": abs(z - zo) / abs(zo),
+            "reference": "FP64 host oracle, same seeded initial state"}
 
 
 def run_qaf(a, world, rank, local):
@@ -314,7 +333,8 @@ def run_qaf(a, world, rank, local):
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(n, a.cpu_sample_steps, a.dtype)
+        line["cpu_baseline"], oracle_run = cpu_baseline(n, a.cpu_sample_steps, a.dtype)
+        line["spectrum_vs_oracle"] = spectrum_vs_oracle(mesh, qaf, oracle_run, a.cpu_sample_steps)
     return line
 
 
