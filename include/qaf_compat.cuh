@@ -312,7 +312,7 @@ namespace qaf_compat {
 inline qaf_params params(Qreal Re, Qreal Er, Qreal lambda, const Qreal* Ra) {
     qaf_params p;
     p.re = Re; p.er = Er; p.rf = 0; p.lambda = lambda; p.alpha = 0; p.alpha_field = Ra;
-    p.dt = 1; p.q_lin = 1; p.advect_omega = 1;
+    p.dt = 1; p.q_lin = 1; p.advect_omega = 1; p.no_dealias = 0;
     return p;
 }
 }  // namespace qaf_compat

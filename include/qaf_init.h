@@ -16,10 +16,18 @@
  * The "random Q" initial state draws N*N values for r1 = Q11 in the physical
  * order i + j*N (x fastest, the reference's layout), then N*N values for
  * r2 = Q12 from the same stream; omega is zero.
+ *
+ * The "coupled" initial state is the smooth one of the reference's coupled
+ * runs (UnitTest/TimeIntegration/couple/couple.cu:4-35): omega = 0,
+ * r1 = 0.2 (sin^2(x+y) - 1/2) + amp u, r2 = 0.2 sin(x+y) cos(x+y) + amp u',
+ * x = i lx/nx, y = j ly/ny, with u, u' ~ U(0, 1) from this stream (draws
+ * i + j nx and nx ny + i + j nx) in place of rand()/RAND_MAX; amp = 1e-3
+ * there.
  */
 #ifndef QAF_INIT_H
 #define QAF_INIT_H
 
+#include <math.h>
 #include <stddef.h>
 #include <stdint.h>
 
@@ -53,6 +61,20 @@ static inline void qaf_random_q_init(uint64_t seed, int nx, int ny, double lo, d
     if (w) for (size_t i = 0; i < n; ++i) w[i] = 0.0;
     if (r1) qaf_fill_uniform(seed, 0, lo, hi, r1, n);
     if (r2) qaf_fill_uniform(seed, n, lo, hi, r2, n);
+}
+
+/* Coupled-run initial state (see the header comment). Any output pointer may be NULL. */
+static inline void qaf_couple_init(uint64_t seed, int nx, int ny, double lx, double ly, double amp,
+                                   double* w, double* r1, double* r2) {
+    size_t n = (size_t)nx * (size_t)ny;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            size_t k = (size_t)i + (size_t)j * (size_t)nx;
+            double s = sin(i * (lx / nx) + j * (ly / ny)), c = cos(i * (lx / nx) + j * (ly / ny));
+            if (w) w[k] = 0.0;
+            if (r1) r1[k] = 0.2 * (s * s - 0.5) + amp * qaf_uniform_at(seed, k, 0.0, 1.0);
+            if (r2) r2[k] = 0.2 * s * c + amp * qaf_uniform_at(seed, n + k, 0.0, 1.0);
+        }
 }
 
 #ifdef __cplusplus

@@ -269,6 +269,18 @@ qaf_status ensure_if(qaf_mesh* m, const qaf_params* p, cudaStream_t st) {
     return QAF_OK;
 }
 
+// the step's truncation of the new state: the 2/3 mask (dealias after stage 4,
+// friction.cu:253-255; keep i <= kx_keep && (j <= ky_lo || j >= ky_hi)), or a
+// mask that keeps every mode (the coupled runs, couple.cu:179-215, never dealias)
+template <class Args>
+void set_mask(Args& a, int N, int no_dealias) {
+    if (no_dealias) {
+        a.kx_keep = N / 2; a.ky_lo = N; a.ky_hi = N;
+    } else {
+        a.kx_keep = (N / 2) * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
+    }
+}
+
 template <typename real>
 StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
     Workspace<real>& w = ws<real>(m);
@@ -279,9 +291,7 @@ StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
     a.lambda = (real)p->lambda; a.ce = (real)(1.0 / (p->er * p->re)); a.alpha = (real)p->alpha;
     a.alpha_field = reinterpret_cast<const real*>(p->alpha_field);
     a.dt = (real)p->dt; a.advect = p->advect_omega ? 1 : 0;
-    a.kx_keep = (nxh - 1) * 2 / 3;
-    a.ky_lo = N / 3;
-    a.ky_hi = N - N / 3 + 1;
+    set_mask(a, N, p->no_dealias);
     for (int f = 0; f < 3; ++f) {
         a.old_m[f] = w.old_m[f]; a.old_n[f] = w.old_n[f]; a.acc_m[f] = w.acc_m[f]; a.acc_n[f] = w.acc_n[f];
         a.nl_m[f] = w.acc_m[f]; a.nl_n[f] = w.acc_n[f];
@@ -1311,7 +1321,7 @@ StageArgs<real> group_args(const qaf_ensemble* e, const EnsGroup<real>& g) {
     a.dkx = (real)(2 * M_PI / e->lx); a.dky = (real)(2 * M_PI / e->ly);
     a.lambda = (real)e->p.lambda; a.ce = (real)(1.0 / (e->p.er * e->p.re)); a.alpha = (real)e->p.alpha;
     a.dt = (real)e->p.dt; a.advect = e->p.advect_omega ? 1 : 0;
-    a.kx_keep = (nxh - 1) * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
+    set_mask(a, N, e->p.no_dealias);
     for (int f = 0; f < 3; ++f) {
         a.old_m[f] = g.w.old_m[f]; a.old_n[f] = g.w.old_n[f]; a.acc_m[f] = g.w.acc_m[f]; a.acc_n[f] = g.w.acc_n[f];
         a.nl_m[f] = g.w.acc_m[f]; a.nl_n[f] = g.w.acc_n[f];
@@ -1823,7 +1833,7 @@ struct OpAdjBackward {
         a.dkx = (real)m->dkx; a.dky = (real)m->dky; a.dt = (real)A->p.dt; a.lambda = (real)A->p.lambda;
         a.ce = (real)(1.0 / (A->p.er * A->p.re));
         a.advect = A->p.advect_omega ? 1 : 0;
-        a.kx_keep = (H + 1 - 1) * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
+        set_mask(a, N, A->p.no_dealias);
         a.tw = w.tw; a.ex = w.ex; a.ey = w.ey;
         for (int c = 0; c < 4; ++c) a.e0[c] = w.e0[c];
         a.Tg = reinterpret_cast<cplx<real>*>(A->Tg); a.Tx = reinterpret_cast<cplx<real>*>(A->Tx);
@@ -2394,7 +2404,7 @@ qaf_status batch_backward(qaf_adjoint_batch* B, const void* const* gT, const dou
     a.dkx = (real)(2 * M_PI / e->lx); a.dky = (real)(2 * M_PI / e->ly); a.dt = (real)p.dt; a.lambda = (real)p.lambda;
     a.ce = (real)(1.0 / (p.er * p.re));
     a.advect = p.advect_omega ? 1 : 0;
-    a.kx_keep = H * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
+    set_mask(a, N, p.no_dealias);
     a.tw = g.w.tw; a.ex = g.w.ex; a.ey = g.w.ey;
     host_if_e0<real>(p.dt, p.re, p.rf, p.q_lin, a.e0);
     a.Tg = reinterpret_cast<cplx<real>*>(B->Tg); a.Tx = reinterpret_cast<cplx<real>*>(B->Tx);

@@ -63,7 +63,8 @@ class MeshDesc(ctypes.Structure):
 class CParams(ctypes.Structure):
     _fields_ = [("re", ctypes.c_double), ("er", ctypes.c_double), ("rf", ctypes.c_double),
                 ("lam", ctypes.c_double), ("alpha", ctypes.c_double), ("alpha_field", ctypes.c_void_p),
-                ("dt", ctypes.c_double), ("q_lin", ctypes.c_double), ("advect_omega", ctypes.c_int)]
+                ("dt", ctypes.c_double), ("q_lin", ctypes.c_double), ("advect_omega", ctypes.c_int),
+                ("no_dealias", ctypes.c_int)]
 
 
 @dataclass
@@ -77,13 +78,15 @@ class Params:
     dt: float = 1e-3
     q_lin: float = 1.0
     advect_omega: int = 1
+    no_dealias: int = 0      # 1: no 2/3 truncation per step (the coupled runs of UnitTest/TimeIntegration)
     alpha_field: Optional[object] = field(default=None, repr=False)   # torch tensor (ny, nx) on the device
 
     def c(self) -> CParams:
         ptr = None
         if self.alpha_field is not None:
             ptr = self.alpha_field.data_ptr()
-        return CParams(self.re, self.er, self.rf, self.lam, self.alpha, ptr, self.dt, self.q_lin, self.advect_omega)
+        return CParams(self.re, self.er, self.rf, self.lam, self.alpha, ptr, self.dt, self.q_lin, self.advect_omega,
+                       self.no_dealias)
 
 
 _lib = None

@@ -31,13 +31,14 @@ class Params(ctypes.Structure):
         ("lx", ctypes.c_double), ("ly", ctypes.c_double),
         ("re", ctypes.c_double), ("er", ctypes.c_double), ("rf", ctypes.c_double), ("lam", ctypes.c_double),
         ("alpha", ctypes.c_double), ("dt", ctypes.c_double), ("q_lin", ctypes.c_double),
-        ("advect_omega", ctypes.c_int), ("emulate_symmetry", ctypes.c_int),
+        ("advect_omega", ctypes.c_int), ("emulate_symmetry", ctypes.c_int), ("no_dealias", ctypes.c_int),
     ]
 
 
 def params(n=128, L=16 * np.pi, re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=1e-3, q_lin=1.0,
-           advect_omega=1, emulate_symmetry=1, ny=None, Ly=None) -> Params:
-    return Params(n, ny or n, L, Ly or L, re, er, rf, lam, alpha, dt, q_lin, advect_omega, emulate_symmetry)
+           advect_omega=1, emulate_symmetry=1, ny=None, Ly=None, no_dealias=0) -> Params:
+    return Params(n, ny or n, L, Ly or L, re, er, rf, lam, alpha, dt, q_lin, advect_omega, emulate_symmetry,
+                  no_dealias)
 
 
 _lib = None
@@ -67,6 +68,8 @@ def lib():
         L.oracle_random_q_init.argtypes = [ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                            ctypes.c_double, dp, dp, dp]
         L.oracle_random_q_init.restype = None
+        L.oracle_couple_init.argtypes = [ctypes.c_ulonglong, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp, dp]
+        L.oracle_couple_init.restype = None
         _lib = L
     return _lib
 
@@ -221,10 +224,30 @@ def random_q_init(seed, n, lo=-0.01, hi=0.01, ny=None):
     return w, r1, r2
 
 
+def couple_init(seed, n, L, amp=1e-3):
+    """Smooth initial state of UnitTest/TimeIntegration/couple/couple.cu:4-35 with
+    seeded noise (qaf_couple_init of include/qaf_init.h): w = 0,
+    r1 = 0.2 (sin^2(x+y) - 1/2) + amp u, r2 = 0.2 sin(x+y) cos(x+y) + amp u'."""
+    np_ = n * n
+    i = np.arange(n)
+    ph = (i[None, :] * (L / n)) + (i[:, None] * (L / n))
+    s, c = np.sin(ph), np.cos(ph)
+    r1 = 0.2 * (s * s - 0.5) + amp * uniform(seed, 0, np_, 0.0, 1.0).reshape(n, n)
+    r2 = 0.2 * s * c + amp * uniform(seed, np_, np_, 0.0, 1.0).reshape(n, n)
+    return np.zeros((n, n)), r1, r2
+
+
 def random_q_init_c(seed, n, lo=-0.01, hi=0.01):
     """The same initial state from the C header (through the oracle library)."""
     w, r1, r2 = (np.empty((n, n)) for _ in range(3))
     lib().oracle_random_q_init(seed, n, n, lo, hi, _p(w), _p(r1), _p(r2))
+    return w, r1, r2
+
+
+def couple_init_c(seed, n, L, amp=1e-3):
+    """The coupled-run initial state from the C header (through the oracle library)."""
+    w, r1, r2 = (np.empty((n, n)) for _ in range(3))
+    lib().oracle_couple_init(seed, n, L, amp, _p(w), _p(r1), _p(r2))
     return w, r1, r2
 
 

@@ -791,7 +791,7 @@ int oracle_step(const oracle_params* p, int integrator, const double* alpha_fiel
                 }
         }
         for (int f = 0; f < 3; ++f)       // dealias + SpecSet(old <- new)
-            for (size_t k = 0; k < ns; ++k) old[f][k] = nw[f][k] * c.m.cutoff[k];
+            for (size_t k = 0; k < ns; ++k) old[f][k] = c.p->no_dealias ? nw[f][k] : nw[f][k] * c.m.cutoff[k];
     }
     return 0;
 }
@@ -840,6 +840,10 @@ int oracle_diagnostics(const oracle_params* p, const double* w, double* energy, 
 void oracle_random_q_init(unsigned long long seed, int nx, int ny, double lo, double hi, double* w, double* r1,
                           double* r2) {
     qaf_random_q_init(seed, nx, ny, lo, hi, w, r1, r2);
+}
+
+void oracle_couple_init(unsigned long long seed, int n, double L, double amp, double* w, double* r1, double* r2) {
+    qaf_couple_init(seed, n, n, L, L, amp, w, r1, r2);
 }
 
 
@@ -915,8 +919,9 @@ int oracle_step_tlm(const oracle_params* p, const double* alpha_field, const dou
             }
         for (int f = 0; f < 3; ++f)
             for (size_t k = 0; k < ns; ++k) {
-                old[f][k] = nw[f][k] * c.m.cutoff[k];
-                dold[f][k] = dnw[f][k] * c.m.cutoff[k];
+                const double keep = c.p->no_dealias ? 1.0 : c.m.cutoff[k];
+                old[f][k] = nw[f][k] * keep;
+                dold[f][k] = dnw[f][k] * keep;
             }
         if (s >= nsteps - loss_window) {
             double z, dz;

@@ -40,6 +40,7 @@ typedef struct {
     double q_lin;          /* L_Q = -k^2 + q_lin (1.0 in the friction solver) */
     int advect_omega;      /* 1: keep -div(u w) in N_w (friction); 0: drop it */
     int emulate_symmetry;  /* 1: BwdTrans symmetrises its input's kx=0 column in place */
+    int no_dealias;        /* 1: steps skip the 2/3 truncation (couple.cu:179-215) */
 } oracle_params;
 
 enum { ORACLE_IFE = 0, ORACLE_IFRK2 = 1, ORACLE_IFRK4 = 2 };
@@ -99,6 +100,8 @@ int oracle_step_tlm(const oracle_params* p, const double* alpha_field, const dou
  * numpy restatement of the generator) */
 void oracle_random_q_init(unsigned long long seed, int nx, int ny, double lo, double hi,
                           double* w, double* r1, double* r2);
+/* the coupled-run initial state of include/qaf_init.h on an n x n grid of side L */
+void oracle_couple_init(unsigned long long seed, int n, double L, double amp, double* w, double* r1, double* r2);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,7 @@ struct Opts {
     uint64_t seed = 0;
     std::string out = "ref";
     int warmup = 3, timed = 10;
+    int dealias = 1;   // 0: the coupled runs' step, no truncation (couple.cu:179-215)
 };
 
 void die(const char* msg) { std::fprintf(stderr, "ref_harness: %s\n", msg); std::exit(2); }
@@ -93,6 +94,7 @@ Opts parse(int argc, char** argv) {
         else if (k == "--out") o.out = v;
         else if (k == "--warmup") o.warmup = std::atoi(v);
         else if (k == "--timed") o.timed = std::atoi(v);
+        else if (k == "--dealias") o.dealias = std::atoi(v);
         else if (k == "--dumps") {
             std::string s = v; size_t p = 0;
             while (p < s.size()) { size_t q = s.find(',', p); if (q == std::string::npos) q = s.size();
@@ -118,6 +120,7 @@ void make_init(const Opts& o, std::vector<double>& w, std::vector<double>& r1, s
     int n = o.n; size_t np = (size_t)n * n;
     w.assign(np, 0); r1.assign(np, 0); r2.assign(np, 0);
     if (o.init == "random") { qaf_random_q_init(o.seed, n, n, -0.01, 0.01, w.data(), r1.data(), r2.data()); return; }
+    if (o.init == "couple") { qaf_couple_init(o.seed, n, n, o.L, o.L, 1e-3, w.data(), r1.data(), r2.data()); return; }
     double dx = o.L / n;
     for (int j = 0; j < n; ++j) for (int i = 0; i < n; ++i) {
         size_t idx = (size_t)i + (size_t)j * n;
@@ -149,13 +152,13 @@ struct Solver {
     Field *p11, *p12, *p21, *Ra, *aux, *aux1;
     Qreal *IFw, *IFwh, *IFr1, *IFr1h, *IFr2, *IFr2h;
     Qreal re, er, rf, lambda, dt;
-    int Nxh, Ny, BSZ;
+    int Nxh, Ny, BSZ, do_dealias;
 
     Solver(const Opts& o) {
         const int BSZ_ = 16;
         mesh = new Mesh(o.n, o.n, o.L, o.L, BSZ_);
         Nxh = mesh->Nxh; Ny = mesh->Ny; BSZ = BSZ_;
-        re = o.re; er = o.er; rf = o.rf; lambda = o.lambda; dt = o.dt;
+        re = o.re; er = o.er; rf = o.rf; lambda = o.lambda; dt = o.dt; do_dealias = o.dealias;
         wold = new Field(mesh); wcurr = new Field(mesh); wnew = new Field(mesh); wnonl = new Field(mesh);
         u = new Field(mesh); v = new Field(mesh);
         r1old = new Field(mesh); r1curr = new Field(mesh); r1new = new Field(mesh); r1nonl = new Field(mesh);
@@ -196,7 +199,8 @@ struct Solver {
         r2nonl_func(r2nonl, wcurr, u, v, r1curr, r2curr, S, lambda, aux, aux1);
     }
 
-    // One IF-RK4 step in the order of friction.cu:213-259.
+    // One IF-RK4 step in the order of friction.cu:213-259; without the dealias
+    // kernels it is the step of the coupled runs (couple.cu:179-215).
     void step() {
         dim3 g = mesh->dimGridsp, b = mesh->dimBlocksp;
         integrate_func0D<<<g, b>>>(wold->spec, wcurr->spec, wnew->spec, IFw, IFwh, Nxh, Ny, BSZ, dt);
@@ -218,9 +222,11 @@ struct Solver {
         integrate_func4D<<<g, b>>>(wold->spec, wcurr->spec, wnew->spec, wnonl->spec, IFw, IFwh, Nxh, Ny, BSZ, dt);
         integrate_func4D<<<g, b>>>(r1old->spec, r1curr->spec, r1new->spec, r1nonl->spec, IFr1, IFr1h, Nxh, Ny, BSZ, dt);
         integrate_func4D<<<g, b>>>(r2old->spec, r2curr->spec, r2new->spec, r2nonl->spec, IFr2, IFr2h, Nxh, Ny, BSZ, dt);
-        dealias<<<g, b>>>(wnew->spec, mesh->cutoff, Nxh, Ny, BSZ);
-        dealias<<<g, b>>>(r1new->spec, mesh->cutoff, Nxh, Ny, BSZ);
-        dealias<<<g, b>>>(r2new->spec, mesh->cutoff, Nxh, Ny, BSZ);
+        if (do_dealias) {
+            dealias<<<g, b>>>(wnew->spec, mesh->cutoff, Nxh, Ny, BSZ);
+            dealias<<<g, b>>>(r1new->spec, mesh->cutoff, Nxh, Ny, BSZ);
+            dealias<<<g, b>>>(r2new->spec, mesh->cutoff, Nxh, Ny, BSZ);
+        }
         SpecSet<<<g, b>>>(wold->spec, wnew->spec, Nxh, Ny, BSZ);
         SpecSet<<<g, b>>>(r1old->spec, r1new->spec, Nxh, Ny, BSZ);
         SpecSet<<<g, b>>>(r2old->spec, r2new->spec, Nxh, Ny, BSZ);

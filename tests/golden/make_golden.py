@@ -4,6 +4,7 @@ reference's unmodified headers; it needs a GPU).
 
     python tests/golden/make_golden.py --run            # on a GPU box: run the driver, then convert
     python tests/golden/make_golden.py --dumps DIR      # convert QAFDUMP1 files already in DIR
+    python tests/golden/make_golden.py --run --only couple64   # one group only
 
 Workloads (all FP64, the reference as shipped; parameters of the friction
 solver with Re = 1, Er = 1, Rf = 0.1, lambda = 0.1, Ra = 1, L = 16 pi unless
@@ -13,6 +14,11 @@ noted; seeded random Q ~ U(-0.01, 0.01), w = 0, generator include/qaf_init.h):
   run32                  IF-RK4 dt = 1e-3, seed 5, states at steps 0 1 2 10 20
   run64                  IF-RK4 dt = 1e-3, seed 0, state at step 100
   run128                 IF-RK4 dt = 1e-3, seed 0, state at step 1000
+  couple64               the coupled runs' step (no dealias, couple.cu:179-215)
+                         and parameters (Re = Er = 0.1, Rf = 7.5e-5, lambda =
+                         0.1, Ra = 0.2, dt = 1e-3) from their smooth initial
+                         state (qaf_couple_init, seed 9) on 64^2, L = 8 pi
+                         (their grid spacing), states at steps 0 1 10 1000
   kat summary            the reference's nonlinear terms for the analytic input
                          sets of UnitTest/Nonlinear/nlterms0-4 (N = 128, L = 2 pi,
                          Re = Er = 0.1, Ra = 0.2), reduced to their deviation from
@@ -36,22 +42,32 @@ import oracle as O  # noqa: E402
 
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 TWO_PI = "6.283185307179586"
+EIGHT_PI = "25.132741228718345"
+GROUPS = ("nl", "run32", "run64", "run128", "kat", "couple64")
+COUPLE_STEPS = (0, 1, 10, 1000)
 
 
-def run_harness(out):
+def run_harness(out, only=GROUPS):
     H = HARNESS
-    cmds = [
-        [H, "nonlinear", "--n", "32", "--init", "random", "--seed", "4", "--out", f"{out}/nl_rand32"],
-        [H, "nonlinear", "--n", "64", "--init", "random", "--seed", "3", "--out", f"{out}/nl_rand64"],
-        [H, "run", "--n", "32", "--steps", "20", "--seed", "5", "--dumps", "0,1,2,10,20", "--out", f"{out}/run32"],
-        [H, "run", "--n", "64", "--steps", "100", "--seed", "0", "--dumps", "0,100", "--out", f"{out}/run64"],
-        [H, "run", "--n", "128", "--steps", "1000", "--seed", "0", "--dumps", "0,1000", "--out", f"{out}/run128"],
-    ]
-    for k in range(5):
-        cmds.append([H, "nonlinear", "--n", "128", "--L", TWO_PI, "--init", f"kat{k}", "--re", "0.1", "--er", "0.1",
-                     "--alpha", "0.2", "--lambda", "0.1", "--rf", "0.000075", "--out", f"{out}/nl_kat{k}"])
-    for c in cmds:
-        subprocess.run(c, check=True)
+    jobs = {
+        "nl": [[H, "nonlinear", "--n", "32", "--init", "random", "--seed", "4", "--out", f"{out}/nl_rand32"],
+               [H, "nonlinear", "--n", "64", "--init", "random", "--seed", "3", "--out", f"{out}/nl_rand64"]],
+        "run32": [[H, "run", "--n", "32", "--steps", "20", "--seed", "5", "--dumps", "0,1,2,10,20",
+                   "--out", f"{out}/run32"]],
+        "run64": [[H, "run", "--n", "64", "--steps", "100", "--seed", "0", "--dumps", "0,100", "--out", f"{out}/run64"]],
+        "run128": [[H, "run", "--n", "128", "--steps", "1000", "--seed", "0", "--dumps", "0,1000",
+                    "--out", f"{out}/run128"]],
+        "kat": [[H, "nonlinear", "--n", "128", "--L", TWO_PI, "--init", f"kat{k}", "--re", "0.1", "--er", "0.1",
+                 "--alpha", "0.2", "--lambda", "0.1", "--rf", "0.000075", "--out", f"{out}/nl_kat{k}"]
+                for k in range(5)],
+        "couple64": [[H, "run", "--n", "64", "--L", EIGHT_PI, "--init", "couple", "--seed", "9", "--re", "0.1",
+                      "--er", "0.1", "--rf", "0.000075", "--lambda", "0.1", "--alpha", "0.2", "--dt", "0.001",
+                      "--dealias", "0", "--steps", str(COUPLE_STEPS[-1]),
+                      "--dumps", ",".join(str(s) for s in COUPLE_STEPS), "--out", f"{out}/couple64"]],
+    }
+    for name in only:
+        for c in jobs[name]:
+            subprocess.run(c, check=True)
 
 
 def kat_fields(k, n=128, L=2 * np.pi):
@@ -83,25 +99,36 @@ def kat_fields(k, n=128, L=2 * np.pi):
             + 0.5 * s(2 * X + 3 * Y))
 
 
-def convert(d):
+def convert(d, only=GROUPS):
     def f(name):
         return O.read_dump(os.path.join(d, name))["fields"]
 
     def save(name, **arrs):
         np.savez_compressed(os.path.join(HERE, name), **arrs)
 
-    for n in (32, 64):
-        i, nl = f(f"nl_rand{n}_in.bin"), f(f"nl_rand{n}_nl.bin")
-        save(f"ref_nl_rand{n}.npz", w=i[0], r1=i[1], r2=i[2], wn=nl[0], r1n=nl[1], r2n=nl[2])
-    arrs = {}
-    for s in (0, 1, 2, 10, 20):
-        st = f(f"run32_s{s}.bin")
-        arrs.update({f"w_{s}": st[0], f"r1_{s}": st[1], f"r2_{s}": st[2]})
-    save("ref_run32.npz", **arrs)
-    st = f("run64_s100.bin")
-    save("ref_run64_s100.npz", w=st[0], r1=st[1], r2=st[2])
-    st = f("run128_s1000.bin")
-    save("ref_run128_s1000.npz", w=st[0], r1=st[1], r2=st[2])
+    def states(prefix, steps):
+        arrs = {}
+        for s in steps:
+            st = f(f"{prefix}_s{s}.bin")
+            arrs.update({f"w_{s}": st[0], f"r1_{s}": st[1], f"r2_{s}": st[2]})
+        return arrs
+
+    if "nl" in only:
+        for n in (32, 64):
+            i, nl = f(f"nl_rand{n}_in.bin"), f(f"nl_rand{n}_nl.bin")
+            save(f"ref_nl_rand{n}.npz", w=i[0], r1=i[1], r2=i[2], wn=nl[0], r1n=nl[1], r2n=nl[2])
+    if "run32" in only:
+        save("ref_run32.npz", **states("run32", (0, 1, 2, 10, 20)))
+    if "run64" in only:
+        st = f("run64_s100.bin")
+        save("ref_run64_s100.npz", w=st[0], r1=st[1], r2=st[2])
+    if "run128" in only:
+        st = f("run128_s1000.bin")
+        save("ref_run128_s1000.npz", w=st[0], r1=st[1], r2=st[2])
+    if "couple64" in only:
+        save("ref_couple64.npz", **states("couple64", COUPLE_STEPS))
+    if "kat" not in only:
+        return
     summary = {}
     for k in range(5):
         fields = kat_fields(k)
@@ -119,13 +146,17 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--run", action="store_true")
     ap.add_argument("--dumps")
+    ap.add_argument("--only", default=",".join(GROUPS), help="comma-separated groups of " + ", ".join(GROUPS))
     a = ap.parse_args()
+    only = tuple(a.only.split(","))
+    if any(g not in GROUPS for g in only):
+        ap.error("unknown group in --only")
     if a.run:
         with tempfile.TemporaryDirectory() as d:
-            run_harness(d)
-            convert(d)
+            run_harness(d, only)
+            convert(d, only)
     elif a.dumps:
-        convert(a.dumps)
+        convert(a.dumps, only)
     else:
         ap.error("give --run or --dumps DIR")
 

@@ -130,7 +130,7 @@ int main(int argc, char** argv) {
 
     qaf_params p;
     p.re = Re; p.er = Er; p.rf = Rf; p.lambda = lambda; p.alpha = alpha; p.alpha_field = nullptr;
-    p.dt = dt; p.q_lin = 1.0; p.advect_omega = 1;
+    p.dt = dt; p.q_lin = 1.0; p.advect_omega = 1; p.no_dealias = 0;
     const qaf_integrator qi = integ == "rk4" ? QAF_IFRK4 : (integ == "rk2" ? QAF_IFRK2 : QAF_IFE);
     qaf_compat::check(qaf_step(mesh->handle, &p, qi, fw, f1, f2, Ns, nullptr), "qaf_step");
     cudaDeviceSynchronize();

@@ -22,8 +22,8 @@ import oracle as O  # noqa: E402
 L = 16 * math.pi
 
 
-def _setup(n, seed, dt=1e-2, advect=1, amp=0.5):
-    p = O.params(n=n, L=L, dt=dt, alpha=1.0, rf=0.1, advect_omega=advect)
+def _setup(n, seed, dt=1e-2, advect=1, amp=0.5, no_dealias=0):
+    p = O.params(n=n, L=L, dt=dt, alpha=1.0, rf=0.1, advect_omega=advect, no_dealias=no_dealias)
     s0 = O.initial_spectra(seed, n, lo=-amp, hi=amp)
     rng = np.random.default_rng(seed + 1000)
     alpha = 1.0 + 0.1 * rng.standard_normal((n, n))
@@ -32,8 +32,9 @@ def _setup(n, seed, dt=1e-2, advect=1, amp=0.5):
     return p, s0, alpha, gT, rng
 
 
-def _qaf_params(qaf, dt, advect=1):
-    return qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=dt, q_lin=1.0, advect_omega=advect)
+def _qaf_params(qaf, dt, advect=1, no_dealias=0):
+    return qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=dt, q_lin=1.0, advect_omega=advect,
+                      no_dealias=no_dealias)
 
 
 def _dev(x, cdt):
@@ -41,11 +42,11 @@ def _dev(x, cdt):
     return torch.as_tensor(np.ascontiguousarray(x)).to(device="cuda", dtype=cdt)
 
 
-def _gpu_grad(qaf, n, dtype, s0, alpha, gT, nsteps, K, window, dt, advect=1, const_alpha=False):
+def _gpu_grad(qaf, n, dtype, s0, alpha, gT, nsteps, K, window, dt, advect=1, const_alpha=False, no_dealias=0):
     import torch
     mesh = qaf.Mesh(n, n, L, L, dtype)
     cdt, rdt = mesh.complex_dtype, mesh.real_dtype
-    p = _qaf_params(qaf, dt, advect)
+    p = _qaf_params(qaf, dt, advect, no_dealias)
     if not const_alpha:
         p.alpha_field = _dev(alpha, rdt)
     adj = qaf.Adjoint(mesh, nsteps, K, window)
@@ -64,12 +65,12 @@ def _tlm_dJ(p, s0, alpha, d, dal, gT, nsteps, window):
     return dL + (_dot(gT, dsT) if gT is not None else 0.0)
 
 
-@pytest.mark.parametrize("advect", [1, 0])
-def test_gradient_matches_oracle_tlm_fp64(cuda, advect):
+@pytest.mark.parametrize("advect,no_dealias", [(1, 0), (0, 0), (1, 1)])
+def test_gradient_matches_oracle_tlm_fp64(cuda, advect, no_dealias):
     import qaf
     n, T, K, Wn, dt = 32, 12, 5, 4, 1e-2
-    p, s0, alpha, gT, rng = _setup(n, 3, dt, advect)
-    loss, _, g, ga = _gpu_grad(qaf, n, qaf.F64, s0, alpha, gT, T, K, Wn, dt, advect)
+    p, s0, alpha, gT, rng = _setup(n, 3, dt, advect, no_dealias=no_dealias)
+    loss, _, g, ga = _gpu_grad(qaf, n, qaf.F64, s0, alpha, gT, T, K, Wn, dt, advect, no_dealias=no_dealias)
     _, _, L_ref, _ = O.step_tlm(p, *s0, *[np.zeros_like(s0[0])] * 3, T, Wn, alpha_field=alpha)
     assert abs(loss - L_ref) <= 1e-10 * abs(L_ref)
     for trial in range(3):

@@ -24,6 +24,18 @@ def test_seeded_generator_numpy_equals_c_header():
     assert np.all(w == 0) and r1.min() >= -0.01 and r1.max() < 0.01 and abs(r2.mean()) < 1e-3
 
 
+def test_couple_init_numpy_equals_c_header():
+    # the smooth initial state of UnitTest/TimeIntegration/couple/couple.cu:4-35
+    for seed, n, L in ((0, 32, 8 * np.pi), (9, 64, 8 * np.pi), (2, 48, 66 * np.pi)):
+        a = O.couple_init(seed, n, L)
+        b = O.couple_init_c(seed, n, L)
+        for x, y in zip(a, b):
+            assert np.abs(x - y).max() <= 1e-16
+    w, r1, r2 = O.couple_init(0, 64, 8 * np.pi)
+    S = 2 * np.sqrt(r1 * r1 + r2 * r2)
+    assert np.all(w == 0) and 0.19 < S.min() and S.max() < 0.21
+
+
 @pytest.mark.parametrize("n", [8, 12, 16, 30, 64, 128, 768])
 def test_transforms_match_numpy(n):
     rng = np.random.default_rng(n)
@@ -197,3 +209,34 @@ def test_diagnostics_definitions():
     for s in range(24):
         k += dk
     assert np.isclose(spec.sum() * 2 * dk * n ** 4, m2[k2 < k * k].sum(), rtol=1e-12)
+
+
+COUPLE = dict(re=0.1, er=0.1, rf=0.000075, lam=0.1, alpha=0.2, dt=0.001)
+
+
+def test_step_without_dealias_is_step_before_truncation():
+    # one step: the friction step's state = the coupled step's state times the 2/3 mask
+    p = O.params(n=32)
+    s0 = O.initial_spectra(1, 32)
+    a = O.step(p, *s0, 1)
+    b = O.step(O.params(n=32, no_dealias=1), *s0, 1)
+    cut = O.tables(p)[3]
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y * cut)
+        assert np.abs(y * (1 - cut)).max() > 0
+
+
+def test_coupled_step_matches_reference_build_64():
+    # the reference's coupled step (couple.cu:179-215: no dealias kernels) with
+    # its parameters, from the reference build's own state 0
+    g = golden("ref_couple64.npz")
+    p = O.params(n=64, L=8 * np.pi, no_dealias=1, **COUPLE)
+    st = (g["w_0"], g["r1_0"], g["r2_0"])
+    prev = 0
+    for s in (1, 10):
+        st = O.step(p, *st, s - prev)
+        prev = s
+        for a, name in zip(st, ("w", "r1", "r2")):
+            assert O.rel_l2(a, g[f"{name}_{s}"]) < 1e-14, (s, name)
+    w0, r10, r20 = (O.fwd(a) for a in O.couple_init(9, 64, 8 * np.pi))
+    assert O.rel_l2(O.hermitian_part(r10), O.hermitian_part(g["r1_0"])) < 1e-15
