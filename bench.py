@@ -16,7 +16,10 @@ Arms:
                   flushed (a 256 MiB write) between timed steps. `e2e`: the same
                   through the public API with host I/O every step — the activity
                   field uploaded from pinned memory (the control input of a
-                  closed-loop run) and the step's energy/enstrophy read back.
+                  closed-loop run; on a copy stream, double-buffered, so that
+                  step k+1's upload overlaps step k) and the step's
+                  energy/enstrophy read back; one event pair around all steps,
+                  uploads, read-backs and L2 flushes.
   reference       the reference's own CUDA build (oracle/_ref, built from its
                   unmodified headers; FP32 through the macro shim, FP64 as
                   shipped) timed on the same GPU with CUDA events. The reference
@@ -292,28 +295,54 @@ def run_qaf(a, world, rank, local):
                 traffic = float(f[1])
 
     # ---- end to end through the public API, host I/O every step ----------
+    # Step k's activity field is uploaded from pinned host memory on a copy
+    # stream into device buffer k % 2 while step k - 1 runs; step k waits for
+    # its upload, and its energy/enstrophy come back asynchronously. One event
+    # pair brackets every step, upload and read-back, and the L2 flushes
+    # between the steps.
     alpha_host = torch.ones((n, n), dtype=mesh.real_dtype).pin_memory()
-    alpha_dev = torch.empty((n, n), dtype=mesh.real_dtype, device="cuda")
-    pe = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=DT, alpha_field=alpha_dev)
-    for _ in range(2):
-        alpha_dev.copy_(alpha_host, non_blocking=True)
-        mesh.advance(pe, 1)
-        mesh.last_diagnostics()
-    barrier(world)
+    alpha_dev = [torch.empty((n, n), dtype=mesh.real_dtype, device="cuda") for _ in range(2)]
+    pe = [qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=DT, alpha_field=alpha_dev[b]) for b in range(2)]
+    main = torch.cuda.current_stream()
+    copy = torch.cuda.Stream()
+    ready = [torch.cuda.Event() for _ in range(2)]
+    free = [torch.cuda.Event() for _ in range(2)]
+
+    def upload(k):
+        b = k % 2
+        with torch.cuda.stream(copy):
+            if k >= 2:
+                copy.wait_event(free[b])           # the step that read this buffer is done
+            alpha_dev[b].copy_(alpha_host, non_blocking=True)
+            ready[b].record(copy)
+
+    def e2e_steps_run(steps, diag_host):
+        upload(0)
+        for k in range(steps):
+            if k + 1 < steps:
+                upload(k + 1)                      # overlaps step k
+            main.wait_event(ready[k % 2])
+            mesh.advance(pe[k % 2], 1)
+            free[k % 2].record(main)
+            mesh.last_diagnostics_async(diag_host[k])
+            if k + 1 < steps:
+                flush.zero_()
+
     e2e_steps = max(10, a.steps // 2)
-    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(e2e_steps)]
-    diag_host = torch.empty((e2e_steps, 2), dtype=torch.float64).pin_memory()   # one slot per step
-    for k, (e0, e1) in enumerate(ev2):
-        flush.zero_()
-        e0.record()
-        alpha_dev.copy_(alpha_host, non_blocking=True)      # H2D: the step's activity field
-        mesh.advance(pe, 1)
-        mesh.last_diagnostics_async(diag_host[k])           # D2H: the step's energy, enstrophy
-        e1.record()
+    diag_host = torch.empty((e2e_steps, 2), dtype=torch.float64).pin_memory()
+    e2e_steps_run(2, diag_host)                    # warm-up of the same pipeline
+    torch.cuda.synchronize()
+    barrier(world)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(main)
+    copy.wait_event(t0)                            # the first upload starts inside the timed region
+    e2e_steps_run(e2e_steps, diag_host)
+    t1.record(main)
+    torch.cuda.synchronize()
     barrier(world)
     mesh.check_finite()
     assert bool(torch.isfinite(diag_host).all()) and bool((diag_host[:, 1] > 0).all())
-    ms2 = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in ev2), world)
+    ms2 = max_over_ranks(t0.elapsed_time(t1), world)
     e2e = {"value": world * n * n * e2e_steps / (ms2 * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": n * n * real_b, "d2h_bytes_per_step": 2 * 8}
 

@@ -74,6 +74,23 @@ struct ColKernel {
     static constexpr int H = N / 2, TEAM = N / E, TILES = H / TW, NTHREADS = TW * TEAM;
     static constexpr int NITEMS = 2 * TILES + 3;
     static constexpr size_t SLAB = (size_t)N * TW;   // complex elements of one slab
+    // elements whose IF factors are fetched ahead of the stage-update stores;
+    // at 1024^2 the extra live registers cost more in spills than they save
+    static constexpr int PF = N >= 1024 ? 1 : (E < 4 ? E : 4);
+    // FP64 at N >= 512: the item code inlined whole, so that the transform
+    // state stays in registers rather than in the call frame (measured 9%
+    // faster at 1024^2; slower for FP32 and smaller FP64 grids, which keep
+    // the compiler's own choice)
+    static constexpr bool INLINE_ITEM = sizeof(real) == 8 && N >= 512;
+    // the diagnostics' per-warp sums meet in shared memory and leave with one
+    // pair of atomics per CTA, except in the FP32 1024^2 kernel, where the
+    // extra barrier measured slower than the per-warp atomics
+    static constexpr bool CTA_DIAG = !(sizeof(real) == 4 && N >= 1024);
+    // IF table value through the read-only path where it is fetched ahead
+    __device__ static real table(const real* p) {
+        if constexpr (PF > 1) return __ldg(p);
+        else return *p;
+    }
     static constexpr int BOXR = N < 256 ? N : 256;    // rows per TMA box (at most 256)
     static constexpr size_t SMEM = 3 * SLAB * sizeof(cplx<real>) + 2 * N * sizeof(cplx<real>) + 4 * sizeof(uint64_t) + 16;
     using FFT = TeamFFT<real, N, E>;
@@ -90,6 +107,7 @@ struct ColKernel {
     bool need_old, need_acc;
     int inst;              // instance of the current item
     size_t io;             // its buffer offset (complex elements)
+    double* red;           // per-warp diagnostic partial sums (the edge table's space, unused by tiles)
 
     __device__ cplx<real>* buf(int b) const { return bufs + (size_t)b * SLAB; }
     __device__ int nG(int f) const { return a.mode == MODE_PROLOGUE ? 0 : (f == 0 ? 3 : 2); }
@@ -158,7 +176,8 @@ struct ColKernel {
     }
 
     // field f of the current tile; its slabs start at s0
-    __device__ void field(int f, int s0) {
+    __device__ void field(int f, int s0) { field_body(f, s0); }
+    __device__ __forceinline__ void field_body(int f, int s0) {
         const int i = T * TW + w;
         const bool edge_col = (i == 0);   // kx = 0 belongs to the edge item
         const real kx = a.dkx * (real)i;
@@ -191,14 +210,28 @@ struct ColKernel {
         } else {
             const int cls = f == 0 ? 0 : 2;
             const real* e0 = a.inst_e0 ? a.inst_e0 + 4 * inst : a.e0;
-            const real exf = a.ex[cls * (H + 1) + i] * e0[cls];
-            const real exh = a.ex[(cls + 1) * (H + 1) + i] * e0[cls + 1];
+            const real exf = table(&a.ex[cls * (H + 1) + i]) * e0[cls];
+            const real exh = table(&a.ex[(cls + 1) * (H + 1) + i]) * e0[cls + 1];
+            // the y factors of PF elements at a time first, through the
+            // read-only path: fetched inside the loop, each load would wait
+            // behind the previous element's stores (the compiler cannot rule
+            // out aliasing), exposing the L2 latency once per element
 #pragma unroll
-            for (int e = 0; e < E; ++e) {
+            for (int c0 = 0; c0 < E; c0 += PF) {
+            real Efs[PF], Ehs[PF];
+#pragma unroll
+            for (int c = 0; c < PF; ++c) {
+                const int j = t + TEAM * (c0 + c);
+                Efs[c] = exf * table(&a.ey[cls * N + j]);
+                Ehs[c] = exh * table(&a.ey[(cls + 1) * N + j]);
+            }
+#pragma unroll
+            for (int c = 0; c < PF; ++c) {
+                const int e = c0 + c;
                 const int j = t + TEAM * e;
                 const int li = j * TW + w;
-                const real Ef = exf * a.ey[cls * N + j];
-                const real Eh = exh * a.ey[(cls + 1) * N + j];
+                const real Ef = Efs[c];
+                const real Eh = Ehs[c];
                 const cplx<real> o = need_old ? ob[li] : mk<real>(0, 0);
                 const cplx<real> ac = need_acc ? ab[li] : mk<real>(0, 0);
                 StageUpdate<real> u = stage_update(a, nl[e], o, ac, Ef, Eh, mask_keep(a, i, j));
@@ -218,6 +251,7 @@ struct ColKernel {
                 }
                 curr[e] = u.curr;
             }
+            }
             if (a.last_stage) {
                 const bool full_warps = (blockDim.x & 31) == 0;
                 if (full_warps) {
@@ -228,7 +262,17 @@ struct ColKernel {
                             zsum += __shfl_xor_sync(0xffffffffu, zsum, o);
                             esum += __shfl_xor_sync(0xffffffffu, esum, o);
                         }
-                        if ((threadIdx.x & 31) == 0) {
+                        if constexpr (CTA_DIAG) {
+                            const int wid = threadIdx.x >> 5;
+                            if ((threadIdx.x & 31) == 0) { red[2 * wid] = zsum; red[2 * wid + 1] = esum; }
+                            __syncthreads();
+                            if (threadIdx.x == 0) {
+                                double z = 0, en = 0;
+                                for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { z += red[2 * k]; en += red[2 * k + 1]; }
+                                double* dg = a.diag + a.diag_istride * inst;
+                                atomicAdd(&dg[0], z); atomicAdd(&dg[1], en);
+                            }
+                        } else if ((threadIdx.x & 31) == 0) {
                             double* dg = a.diag + a.diag_istride * inst;
                             atomicAdd(&dg[0], zsum); atomicAdd(&dg[1], esum);
                         }
@@ -268,7 +312,8 @@ struct ColKernel {
     }
 
     // a regular item: the fields fa_ (and fb_ >= 0) of tile T_ of instance inst_
-    __device__ void item(int fa_, int fb_, int T_, int inst_) {
+    __device__ void item(int fa_, int fb_, int T_, int inst_) { item_body(fa_, fb_, T_, inst_); }
+    __device__ __forceinline__ void item_body(int fa_, int fb_, int T_, int inst_) {
         fa = fa_; fb = fb_; T = T_;
         inst = inst_;
         io = (size_t)inst_ * a.istride;
@@ -281,8 +326,13 @@ struct ColKernel {
         nseq = per_a + (fb >= 0 ? per_field(fb) : 0);
         next = 0;
         issue_upto(3);
-        field(fa, 0);
-        if (fb >= 0) field(fb, per_a);
+        if constexpr (INLINE_ITEM) {
+            field_body(fa, 0);
+            if (fb >= 0) field_body(fb, per_a);
+        } else {
+            field(fa, 0);
+            if (fb >= 0) field(fb, per_a);
+        }
         __syncthreads();   // buffers free for the next item
     }
 };
@@ -398,38 +448,58 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int in
             const bool need_acc = (a.integrator == INT_IFRK4 && a.stage >= 2) || (a.integrator == INT_IFRK2 && a.stage == 2);
             const int cls = f == 0 ? 0 : 2;
             bool bad = false;
+            const real* e0 = a.inst_e0 ? a.inst_e0 + 4 * inst : a.e0;
+            const real f0 = e0[cls], f1 = e0[cls + 1];
+            // chunks of C elements: the chunk's factors and state are read
+            // before any of its stores, so that their loads overlap (one
+            // element at a time at 1024^2, where the registers are short)
+            constexpr int C = N >= 1024 ? 1 : (E < 4 ? E : 4);
+            auto table = [](const real* p) -> real {
+                if constexpr (C > 1) return __ldg(p);
+                else return *p;
+            };
+            const real x0f = table(&a.ex[cls * (H + 1)]), x0h = table(&a.ex[(cls + 1) * (H + 1)]);
+            const real xHf = table(&a.ex[cls * (H + 1) + H]), xHh = table(&a.ex[(cls + 1) * (H + 1) + H]);
 #pragma unroll
-            for (int e = 0; e < E; ++e) {
-                const int j = t + TEAM * e;
-                const real ky = ky_of<real>(j, N, a.dky);
-                const real* e0 = a.inst_e0 ? a.inst_e0 + 4 * inst : a.e0;
-                const real eyf = a.ey[cls * N + j] * e0[cls], eyh = a.ey[(cls + 1) * N + j] * e0[cls + 1];
-                // column kx = 0
-                {
-                    const size_t idx = (size_t)j * TW;   // tile 0, column 0
-                    const real Ef = a.ex[cls * (H + 1)] * eyf, Eh = a.ex[(cls + 1) * (H + 1)] * eyh;
-                    const cplx<real> o = need_old ? om[idx] : mk<real>(0, 0);
-                    const cplx<real> ac = need_acc ? am[idx] : mk<real>(0, 0);
-                    StageUpdate<real> u = stage_update(a, ctab[j], o, ac, Ef, Eh, mask_keep(a, 0, j));
-                    if (u.write_acc) am[idx] = u.acc;
-                    if (u.write_old) {
-                        om[idx] = u.acc;
-                        bad |= !(isfinite(u.acc.x) && isfinite(u.acc.y));
-                    }
-                    ctab[j] = u.curr;
+            for (int c0 = 0; c0 < E; c0 += C) {
+                real eyf[C], eyh[C];
+                cplx<real> o0[C], a0[C], oH[C], aH[C];
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const int j = t + TEAM * (c0 + c);
+                    eyf[c] = table(&a.ey[cls * N + j]) * f0;
+                    eyh[c] = table(&a.ey[(cls + 1) * N + j]) * f1;
+                    o0[c] = need_old ? om[(size_t)j * TW] : mk<real>(0, 0);   // tile 0, column 0
+                    a0[c] = need_acc ? am[(size_t)j * TW] : mk<real>(0, 0);
+                    oH[c] = need_old ? on[j] : mk<real>(0, 0);
+                    aH[c] = need_acc ? an[j] : mk<real>(0, 0);
                 }
-                // column kx = N/2
-                {
-                    const real Ef = a.ex[cls * (H + 1) + H] * eyf, Eh = a.ex[(cls + 1) * (H + 1) + H] * eyh;
-                    const cplx<real> o = need_old ? on[j] : mk<real>(0, 0);
-                    const cplx<real> ac = need_acc ? an[j] : mk<real>(0, 0);
-                    StageUpdate<real> u = stage_update(a, ctab[N + j], o, ac, Ef, Eh, mask_keep(a, H, j));
-                    if (u.write_acc) an[j] = u.acc;
-                    if (u.write_old) {
-                        on[j] = u.acc;
-                        bad |= !(isfinite(u.acc.x) && isfinite(u.acc.y));
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const int j = t + TEAM * (c0 + c);
+                    // column kx = 0
+                    {
+                        const size_t idx = (size_t)j * TW;
+                        const real Ef = x0f * eyf[c], Eh = x0h * eyh[c];
+                        StageUpdate<real> u = stage_update(a, ctab[j], o0[c], a0[c], Ef, Eh, mask_keep(a, 0, j));
+                        if (u.write_acc) am[idx] = u.acc;
+                        if (u.write_old) {
+                            om[idx] = u.acc;
+                            bad |= !(isfinite(u.acc.x) && isfinite(u.acc.y));
+                        }
+                        ctab[j] = u.curr;
                     }
-                    ctab[N + j] = u.curr;
+                    // column kx = N/2
+                    {
+                        const real Ef = xHf * eyf[c], Eh = xHh * eyh[c];
+                        StageUpdate<real> u = stage_update(a, ctab[N + j], oH[c], aH[c], Ef, Eh, mask_keep(a, H, j));
+                        if (u.write_acc) an[j] = u.acc;
+                        if (u.write_old) {
+                            on[j] = u.acc;
+                            bad |= !(isfinite(u.acc.x) && isfinite(u.acc.y));
+                        }
+                        ctab[N + j] = u.curr;
+                    }
                 }
             }
             if (a.last_stage && bad && a.flags) atomicOr(a.flags, FLAG_NONFINITE);
@@ -504,6 +574,7 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
     typename K::FFT fft;
     fft.template init<N>(t, a.tw);
     K k{a, fft, t, w, bufs, mbar, 0u, 0, 0, 0, 0, 0, 0, false, false};
+    k.red = reinterpret_cast<double*>(ctab);
     // item q of the launch: kind-major over instances (all r1+r2 tiles of all
     // instances first, then the w tiles, then the edge columns)
     const int total = K::NITEMS * a.ninst;
@@ -514,9 +585,13 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
         __syncthreads();
         if (q >= total) break;
         const int local = q / a.ninst, inst = q % a.ninst;
-        if (local < K::TILES) k.item(1, 2, local, inst);
-        else if (local < 2 * K::TILES) k.item(0, -1, local - K::TILES, inst);
-        else {
+        if (local < K::TILES) {
+            if constexpr (K::INLINE_ITEM) k.item_body(1, 2, local, inst);
+            else k.item(1, 2, local, inst);
+        } else if (local < 2 * K::TILES) {
+            if constexpr (K::INLINE_ITEM) k.item_body(0, -1, local - K::TILES, inst);
+            else k.item(0, -1, local - K::TILES, inst);
+        } else {
             col_edge<real, N, TW, E>(a, local - 2 * K::TILES, inst, t, w, bufs, ctab);
             __syncthreads();
         }
@@ -649,7 +724,7 @@ struct RowKernel {
         for (int e = 0; e < E; ++e) o[t + TEAM * e] = kp(slot, e);
     }
     __device__ real alpha_at(int e) const {
-        if (a.alpha_field) return a.alpha_field[a.alpha_istride * inst + (size_t)n * N + t + TEAM * e];
+        if (a.alpha_field) return __ldg(&a.alpha_field[a.alpha_istride * inst + (size_t)n * N + t + TEAM * e]);
         return a.inst_alpha ? a.inst_alpha[inst] : a.alpha;
     }
     __device__ real S_at(int e) const {
@@ -678,9 +753,14 @@ struct RowKernel {
         //    single + Rar + cross of p11func/p12func/p21func (Qsolver.cuh:75-151)
         c2r(PF_LR1, PF_LR2, v);
         dump(PF_LR1, v, false); dump(PF_LR2, v, true);
+        // the activities first: read in the loop, each would wait behind the
+        // previous element's shared-memory stores (possible aliasing)
+        real alv[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) alv[e] = alpha_at(e);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const real r1 = kp(0, e), r2 = kp(1, e), L1 = v[e].x, L2 = v[e].y, al = alpha_at(e);
+            const real r1 = kp(0, e), r2 = kp(1, e), L1 = v[e].x, L2 = v[e].y, al = alv[e];
             const real S = 2 * sqrt(r1 * r1 + r2 * r2);
             const real sgl = lam * S * (S * S - 1);
             const real sg2 = -lam * L2 * S + sgl * r2;
