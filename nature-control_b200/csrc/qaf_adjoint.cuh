@@ -133,23 +133,43 @@ __device__ __forceinline__ cplx<real> adj_emit(int q, cplx<real> lw, cplx<real> 
     }
 }
 
-// The RK4 adjoint recursion at one spectral point of field f. cb: the VJP of
-// the stage (unused at stage 0); returns the nonlinear adjoint kb of the
-// stage before. lossg: the loss gradient of the state completed here.
+// The RK4 adjoint recursion at one spectral point of field f, in two parts:
+// adj_rk_load reads the accumulators the stage needs — sbar (stage 0), sacc
+// (stage 1), abar and sacc (stages 2-4) — and adj_rk_apply updates them. The
+// callers load every field before any field's stores, so that the loads
+// overlap (the compiler cannot move them across stores it cannot prove
+// disjoint). cb: the VJP of the stage (unused at stage 0); adj_rk_apply
+// returns the nonlinear adjoint kb of the stage before. lossg: the loss
+// gradient of the state completed here.
 template <typename real>
-__device__ __forceinline__ cplx<real> adj_rk(const AdjArgs<real>& a, int f, size_t idx, cplx<real> cb, real E,
-                                             real Eh, bool keep, cplx<real> lossg) {
+struct AdjHeld {
+    cplx<real> x, y;
+};
+
+template <typename real>
+__device__ __forceinline__ AdjHeld<real> adj_rk_load(const AdjArgs<real>& a, int f, size_t idx) {
+    AdjHeld<real> h;
+    h.y = mk<real>(0, 0);
+    if (a.stage == 0) h.x = pick3(a.sbar, f)[idx];
+    else if (a.stage == 1) h.x = pick3(a.sacc, f)[idx];
+    else { h.x = pick3(a.abar, f)[idx]; h.y = pick3(a.sacc, f)[idx]; }
+    return h;
+}
+
+template <typename real>
+__device__ __forceinline__ cplx<real> adj_rk_apply(const AdjArgs<real>& a, int f, size_t idx, AdjHeld<real> h,
+                                                   cplx<real> cb, real E, real Eh, bool keep, cplx<real> lossg) {
     const real dt = a.dt;
     const real sixth = (real)(1.0 / 6.0), third = (real)(1.0 / 3.0), half = (real)0.5;
     cplx<real> sb;
     if (a.stage == 0) {
-        sb = cadd(pick3(a.sbar, f)[idx], lossg);
+        sb = cadd(h.x, lossg);
     } else if (a.stage == 1) {
-        sb = cadd(cadd(pick3(a.sacc, f)[idx], cb), lossg);
+        sb = cadd(cadd(h.x, cb), lossg);
         pick3(a.sbar, f)[idx] = sb;
     } else {
-        const cplx<real> av = pick3(a.abar, f)[idx];
-        cplx<real> sc = pick3(a.sacc, f)[idx];
+        const cplx<real> av = h.x;
+        cplx<real> sc = h.y;
         cplx<real> kb;
         if (a.stage == 4) {
             sc = cadd(sc, cscale(cb, E));
@@ -176,8 +196,8 @@ template <typename real, int N>
 __device__ __forceinline__ void adj_factors(const AdjArgs<real>& a, int f, int i, int j, real& E, real& Eh) {
     constexpr int H = N / 2;
     const int cls = f == 0 ? 0 : 2;
-    E = a.ex[cls * (H + 1) + i] * a.e0[cls] * a.ey[cls * N + j];
-    Eh = a.ex[(cls + 1) * (H + 1) + i] * a.e0[cls + 1] * a.ey[(cls + 1) * N + j];
+    E = __ldg(&a.ex[cls * (H + 1) + i]) * a.e0[cls] * __ldg(&a.ey[cls * N + j]);
+    Eh = __ldg(&a.ex[(cls + 1) * (H + 1) + i]) * a.e0[cls + 1] * __ldg(&a.ey[(cls + 1) * N + j]);
 }
 
 template <typename real>
@@ -237,11 +257,17 @@ __device__ void adj_col_edge(const AdjArgs<real>& a, const TeamFFT<real, N, E>& 
                 }
                 const bool keep = adj_keep(a, i, j);
                 cplx<real> cb[3] = {cscale(cw[e], sc), cscale(c1[e], sc), cscale(c2[e], sc)};
+                real Ef[3], Eh[3];
+                AdjHeld<real> held[3];
 #pragma unroll
                 for (int f = 0; f < 3; ++f) {
-                    real Ef, Eh;
-                    adj_factors<real, N>(a, f, i, j, Ef, Eh);
-                    const cplx<real> kb = adj_rk(a, f, idx, cb[f], Ef, Eh, keep, f == 0 ? lossg : mk<real>(0, 0));
+                    adj_factors<real, N>(a, f, i, j, Ef[f], Eh[f]);
+                    held[f] = adj_rk_load(a, f, idx);
+                }
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                    const cplx<real> kb = adj_rk_apply(a, f, idx, held[f], cb[f], Ef[f], Eh[f], keep,
+                                                       f == 0 ? lossg : mk<real>(0, 0));
                     a.edge[(size_t)(f * 2 + c) * N + j] = kb;
                 }
             }
@@ -328,12 +354,13 @@ __global__ void __launch_bounds__(W * (N / E)) adj_col_kernel(const __grid_const
             const size_t idx = (size_t)j * NXH + i;
             const bool keep = adj_keep(a, i, j);
             const cplx<real> lossg = a.wstate ? cscale(a.wstate[idx], 2 * a.loss_w * n4) : mk<real>(0, 0);
-            real Ef, Eh;
-            adj_factors<real, N>(a, 0, i, j, Ef, Eh);
-            cw[e] = adj_rk(a, 0, idx, cscale(cw[e], sc), Ef, Eh, keep, lossg);
+            real Ef0, Eh0, Ef, Eh;
+            adj_factors<real, N>(a, 0, i, j, Ef0, Eh0);
             adj_factors<real, N>(a, 1, i, j, Ef, Eh);
-            c1[e] = adj_rk(a, 1, idx, cscale(c1[e], sc), Ef, Eh, keep, mk<real>(0, 0));
-            c2[e] = adj_rk(a, 2, idx, cscale(c2[e], sc), Ef, Eh, keep, mk<real>(0, 0));
+            const AdjHeld<real> h0 = adj_rk_load(a, 0, idx), h1 = adj_rk_load(a, 1, idx), h2 = adj_rk_load(a, 2, idx);
+            cw[e] = adj_rk_apply(a, 0, idx, h0, cscale(cw[e], sc), Ef0, Eh0, keep, lossg);
+            c1[e] = adj_rk_apply(a, 1, idx, h1, cscale(c1[e], sc), Ef, Eh, keep, mk<real>(0, 0));
+            c2[e] = adj_rk_apply(a, 2, idx, h2, cscale(c2[e], sc), Ef, Eh, keep, mk<real>(0, 0));
         }
     }
     if (!a.emit) return;
@@ -414,13 +441,17 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
             const size_t idx = (size_t)j * NXH + i2;
             const bool keep = adj_keep(a, i2, j);
             const cplx<real> lossg = wst ? cscale(wst[idx], 2 * lw * n2 * n2) : mk<real>(0, 0);
+            real Ef[3], Eh[3];
+            AdjHeld<real> held[3];
 #pragma unroll
             for (int g = 0; g < 3; ++g) {
-                real Ef, Eh;
-                adj_factors<real, N>(a, g, i2, j, Ef, Eh);
-                sm[(size_t)g * SPAN + j * W + w2] =
-                    adj_rk(a, g, so + idx, cscale(cb[g], 2 * n2), Ef, Eh, keep, g == 0 ? lossg : mk<real>(0, 0));
+                adj_factors<real, N>(a, g, i2, j, Ef[g], Eh[g]);
+                held[g] = adj_rk_load(a, g, so + idx);
             }
+#pragma unroll
+            for (int g = 0; g < 3; ++g)
+                sm[(size_t)g * SPAN + j * W + w2] = adj_rk_apply(a, g, so + idx, held[g], cscale(cb[g], 2 * n2), Ef[g],
+                                                                 Eh[g], keep, g == 0 ? lossg : mk<real>(0, 0));
         }
         __syncthreads();
         if (!a.emit) return;
@@ -485,13 +516,17 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
             lossg = cscale(P, lw * n2 * n2);
         }
         const bool keep = adj_keep(a, i, j);
+        real Ef[3], Eh[3];
+        AdjHeld<real> held[3];
 #pragma unroll
         for (int g = 0; g < 3; ++g) {
-            real Ef, Eh;
-            adj_factors<real, N>(a, g, i, j, Ef, Eh);
-            sm[(size_t)g * SPAN + c * N + j] =
-                adj_rk(a, g, so + idx, cscale(cb[g], n2), Ef, Eh, keep, g == 0 ? lossg : mk<real>(0, 0));
+            adj_factors<real, N>(a, g, i, j, Ef[g], Eh[g]);
+            held[g] = adj_rk_load(a, g, so + idx);
         }
+#pragma unroll
+        for (int g = 0; g < 3; ++g)
+            sm[(size_t)g * SPAN + c * N + j] = adj_rk_apply(a, g, so + idx, held[g], cscale(cb[g], n2), Ef[g], Eh[g], keep,
+                                                            g == 0 ? lossg : mk<real>(0, 0));
     }
     __syncthreads();
     if (!a.emit) return;
