@@ -2,7 +2,10 @@
 // autotuner (see qaf_variants.cuh): column kernel with 16 (or, at 64^2, 4)
 // values per thread of the y-FFT instead of 8, or a tighter register budget
 // (more resident CTAs); row kernel with fewer rows per CTA (more CTAs for
-// small grids), 16 values per thread of the x-FFT, or a tighter register budget.
+// small grids), 16 values per thread of the x-FFT, or a tighter register budget
+// (row:e8r1m7 at 1024^2: one row per CTA at 7 CTAs per SM, so the 1024 rows
+// fit the 1036 slots of one wave; 72 registers with spills, within 1% of the
+// built-in two-row shape in same-box A/B runs).
 #include "qaf_kernels.cuh"
 #include "qaf_variants.cuh"
 
@@ -65,7 +68,7 @@ StepVariant<float> v256[] = {make<ColV<256, 16>>("col:e16", 0), make<ColV<256, 8
                              make<ColV<256, 8, 6>>("col:e8m6", 0), make<RowV<256, 8, 2>>("row:e8r2", 1),
                              make<RowV<256, 16, 8>>("row:e16r8", 1), make<RowV<256, 8, 8, 3>>("row:e8r8m3", 1)};
 StepVariant<float> v1024[] = {make<ColV<1024, 16>>("col:e16", 0), make<RowV<1024, 8, 1>>("row:e8r1", 1),
-                              make<RowV<1024, 16, 4>>("row:e16r4", 1)};
+                              make<RowV<1024, 16, 4>>("row:e16r4", 1), make<RowV<1024, 8, 1, 7>>("row:e8r1m7", 1)};
 
 }  // namespace
 
