@@ -130,3 +130,28 @@ def test_coupled_smooth_run_keeps_order_bounded(cuda, dtype):
     assert smax <= 1.04
     assert top > 1.0                           # the ordered state formed and persists
     assert sum(late) / len(late) < 0.016
+
+
+@pytest.mark.parametrize("dtype,bar", [(qaf.F64, 1e-12), (qaf.F32, 1e-4)])
+def test_q_only_run_against_oracle(cuda, dtype, bar):
+    # decoupledQ/Qpure.cu:80-238: w frozen at its initial 0, Q alone
+    # (lambda = 0.1, Re = 40, dt = 0.02, L = 2 pi, r1 = 0.9 (sin^2(x+y) - 1/2),
+    # r2 = 0.9 sin(x+y) cos(x+y)). With the active stress off (Er = inf, so
+    # 1/(Er Re) = 0, and Ra = 0) w stays exactly 0 and u = v = 0: that run.
+    # (Its stage 4 calls integrate_func2D where integrate_func4D belongs,
+    # Qpure.cu:212-213; the scheme here is the correct IF-RK4.)
+    n, L = 64, 2 * math.pi
+    x = np.arange(n) * L / n
+    X, Y = np.meshgrid(x, x)
+    s0 = [O.fwd(np.zeros((n, n))), O.fwd(0.9 * (np.sin(X + Y) ** 2 - 0.5)), O.fwd(0.9 * np.sin(X + Y) * np.cos(X + Y))]
+    kw = dict(re=40.0, rf=0.0, lam=0.1, alpha=0.0, dt=0.02)
+    ref = O.step(O.params(n=n, L=L, er=float("inf"), **kw), *s0, 50)
+    m = qaf.Mesh(n, lx=L, dtype=dtype)
+    st = [dev(a, m) for a in s0]
+    m.step(qaf.Params(er=float("inf"), **kw), *st, nsteps=50)
+    # w stays 0 up to roundoff: the row pass transforms two real fields as one
+    # complex FFT, so w's physical values carry its partner's rounding (the
+    # oracle, transforming each field alone, keeps it exactly 0)
+    assert float(st[0].abs().max()) <= bar * float(st[1].abs().max())
+    for t, o in zip(st[1:], ref[1:]):
+        assert O.rel_l2(host(t), o) < bar
