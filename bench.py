@@ -98,6 +98,9 @@ def parse():
     ap.add_argument("--no-fd", action="store_true", help="adjoint workload: skip the finite-difference check")
     ap.add_argument("--no-tune", action="store_true",
                     help="ensemble, adjoint and control workloads: keep the built-in launch shapes")
+    ap.add_argument("--shapes", default=None,
+                    help="adjoint workload: launch shapes to use instead of tuning, e.g. col:e8m4,row:e8r2 "
+                         "(to profile the shapes a tuned run reported)")
     ap.add_argument("--instances", type=int, default=ENS_COUNT)
     return ap.parse_args()
 
@@ -605,7 +608,11 @@ def run_adjoint(a, world, rank, local):
         return mesh, p, mesh.random_q(SEED)
 
     shapes = "col:default row:default"
-    if not a.no_tune:                         # launch shapes for this grid (untimed)
+    if a.shapes:                              # given shapes, e.g. those a tuned run reported
+        col, row = (s.strip() for s in a.shapes.split(","))
+        qaf.set_variant(n, qaf.F32, False, col, row)
+        shapes = f"{col} {row}"
+    elif not a.no_tune:                       # launch shapes for this grid (untimed)
         shapes, _ = qaf.autotune(n, qaf.F32, 1, None)
     mesh, p, s0 = setup(qaf.F32)
     adj = qaf.Adjoint(mesh, T, K, Wn)
