@@ -3,6 +3,7 @@ energy spectrum stay within 1% of the FP64 path's (the FP64 path matches the
 reference's own build to 1e-10 over 1000 steps, test_gpu_parity.py). Past a
 few thousand steps pointwise agreement is not expected; statistics are."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -10,9 +11,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _run(qaf, dtype, n, steps, chunk, nshells):
+def _run(qaf, dtype, n, steps, chunk, nshells, dt=1e-3):
     m = qaf.Mesh(n, lx=16 * math.pi, dtype=dtype)
-    p = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=1e-3)
+    p = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=dt)
     m.load(*m.random_q(1))
     diags, specs = [], []
     for c in range(steps // chunk):
@@ -37,4 +38,24 @@ def test_fp32_statistics_within_one_percent_of_fp64(cuda):
     assert abs(e32 - e64) <= 0.01 * e64, (e32, e64)
     big = s64 > 1e-3 * s64.max()          # the shells that carry the energy
     rel = np.abs(s32[big] - s64[big]) / s64[big]
+    assert rel.max() <= 0.01, rel.max()
+
+
+@pytest.mark.skipif(os.environ.get("QAF_LONG") != "1", reason="minutes of GPU time: set QAF_LONG=1")
+def test_fp32_statistics_at_1024_within_one_percent_of_fp64(cuda):
+    # the throughput configuration (1024^2, L = 16 pi, dt = 5e-4) over 60000
+    # steps (30 time units); statistics over the second half
+    import qaf
+    n, steps, chunk, nshells = 1024, 60000, 1000, 80
+    d32, s32 = _run(qaf, qaf.F32, n, steps, chunk, nshells, dt=5e-4)
+    d64, s64 = _run(qaf, qaf.F64, n, steps, chunk, nshells, dt=5e-4)
+    h = len(d64) // 2
+    e32, z32 = d32[h:, 0].mean(), d32[h:, 1].mean()
+    e64, z64 = d64[h:, 0].mean(), d64[h:, 1].mean()
+    big = s64 > 1e-3 * s64.max()
+    rel = np.abs(s32[big] - s64[big]) / s64[big]
+    print(f"1024^2: enstrophy {z32:.6e} / {z64:.6e}, energy {e32:.6e} / {e64:.6e}, "
+          f"max shell deviation {rel.max():.3e} over {int(big.sum())} shells")
+    assert abs(z32 - z64) <= 0.01 * z64, (z32, z64)
+    assert abs(e32 - e64) <= 0.01 * e64, (e32, e64)
     assert rel.max() <= 0.01, rel.max()
