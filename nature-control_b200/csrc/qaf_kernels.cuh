@@ -212,45 +212,46 @@ struct ColKernel {
             const real* e0 = a.inst_e0 ? a.inst_e0 + 4 * inst : a.e0;
             const real exf = table(&a.ex[cls * (H + 1) + i]) * e0[cls];
             const real exh = table(&a.ex[(cls + 1) * (H + 1) + i]) * e0[cls + 1];
-            // the y factors of PF elements at a time first, through the
-            // read-only path: fetched inside the loop, each load would wait
-            // behind the previous element's stores (the compiler cannot rule
-            // out aliasing), exposing the L2 latency once per element
+            // the y factors of PF elements at a time first (through the
+            // read-only path when PF > 1): fetched inside the loop, each load
+            // would wait behind the previous element's stores (the compiler
+            // cannot rule out aliasing), exposing the L2 latency once per
+            // element
 #pragma unroll
             for (int c0 = 0; c0 < E; c0 += PF) {
-            real Efs[PF], Ehs[PF];
+                real Efs[PF], Ehs[PF];
 #pragma unroll
-            for (int c = 0; c < PF; ++c) {
-                const int j = t + TEAM * (c0 + c);
-                Efs[c] = exf * table(&a.ey[cls * N + j]);
-                Ehs[c] = exh * table(&a.ey[(cls + 1) * N + j]);
-            }
+                for (int c = 0; c < PF; ++c) {
+                    const int j = t + TEAM * (c0 + c);
+                    Efs[c] = exf * table(&a.ey[cls * N + j]);
+                    Ehs[c] = exh * table(&a.ey[(cls + 1) * N + j]);
+                }
 #pragma unroll
-            for (int c = 0; c < PF; ++c) {
-                const int e = c0 + c;
-                const int j = t + TEAM * e;
-                const int li = j * TW + w;
-                const real Ef = Efs[c];
-                const real Eh = Ehs[c];
-                const cplx<real> o = need_old ? ob[li] : mk<real>(0, 0);
-                const cplx<real> ac = need_acc ? ab[li] : mk<real>(0, 0);
-                StageUpdate<real> u = stage_update(a, nl[e], o, ac, Ef, Eh, mask_keep(a, i, j));
-                if (!edge_col) {
-                    if (u.write_acc) am[li] = u.acc;
-                    if (u.write_old) {
-                        om[li] = u.acc;
-                        bad |= !(isfinite(u.acc.x) && isfinite(u.acc.y));
-                        if (f == 0 && a.diag) {
-                            const real ky = ky_of<real>(j, N, a.dky);
-                            const double k2 = (double)kx * kx + (double)ky * ky;
-                            const double m2 = (double)u.acc.x * u.acc.x + (double)u.acc.y * u.acc.y;
-                            zsum += 2.0 * m2;
-                            if (k2 > 0) esum += 2.0 * m2 / k2;
+                for (int c = 0; c < PF; ++c) {
+                    const int e = c0 + c;
+                    const int j = t + TEAM * e;
+                    const int li = j * TW + w;
+                    const real Ef = Efs[c];
+                    const real Eh = Ehs[c];
+                    const cplx<real> o = need_old ? ob[li] : mk<real>(0, 0);
+                    const cplx<real> ac = need_acc ? ab[li] : mk<real>(0, 0);
+                    StageUpdate<real> u = stage_update(a, nl[e], o, ac, Ef, Eh, mask_keep(a, i, j));
+                    if (!edge_col) {
+                        if (u.write_acc) am[li] = u.acc;
+                        if (u.write_old) {
+                            om[li] = u.acc;
+                            bad |= !(isfinite(u.acc.x) && isfinite(u.acc.y));
+                            if (f == 0 && a.diag) {
+                                const real ky = ky_of<real>(j, N, a.dky);
+                                const double k2 = (double)kx * kx + (double)ky * ky;
+                                const double m2 = (double)u.acc.x * u.acc.x + (double)u.acc.y * u.acc.y;
+                                zsum += 2.0 * m2;
+                                if (k2 > 0) esum += 2.0 * m2 / k2;
+                            }
                         }
                     }
+                    curr[e] = u.curr;
                 }
-                curr[e] = u.curr;
-            }
             }
             if (a.last_stage) {
                 const bool full_warps = (blockDim.x & 31) == 0;
