@@ -65,7 +65,8 @@ typedef struct {
     double q_lin;       /* L_Q = -k^2 + q_lin (hard-wired 1.0 in r1lin_func/r2lin_func :32-54) */
     int advect_omega;   /* 1: keep -div(u w) in N_w (friction variant); 0: drop it (beginning2) */
     int no_dealias;     /* 0: 2/3 truncation of the state after every step (friction.cu:253-255);
-                           1: none, as the coupled runs (UnitTest/TimeIntegration/couple/couple.cu:179-215) */
+                           1: none, as the coupled runs (UnitTest/TimeIntegration/couple/couple.cu:179-215);
+                           2: of w only, as UnitTest/TimeIntegration/dealias/couple.cu:226-229 */
 } qaf_params;
 
 typedef struct qaf_mesh qaf_mesh;

@@ -50,6 +50,7 @@ template <typename real>
 struct AdjArgs {
     real dkx, dky, dt, lambda, ce;
     int advect, kx_keep, ky_lo, ky_hi;
+    int trunc;                 // fields the 2/3 mask truncates: bit f for field f
     const cplx<real>* tw;
     const real* ex;
     const real* ey;
@@ -201,8 +202,8 @@ __device__ __forceinline__ void adj_factors(const AdjArgs<real>& a, int f, int i
 }
 
 template <typename real>
-__device__ __forceinline__ bool adj_keep(const AdjArgs<real>& a, int i, int j) {
-    return i <= a.kx_keep && (j <= a.ky_lo || j >= a.ky_hi);
+__device__ __forceinline__ bool adj_keep(const AdjArgs<real>& a, int f, int i, int j) {
+    return !((a.trunc >> f) & 1) || (i <= a.kx_keep && (j <= a.ky_lo || j >= a.ky_hi));
 }
 
 // kx = 0 and kx = N/2 columns (packed in slot 0 of the T arrays as DC + i Nyquist), by the first team of the last block
@@ -255,7 +256,6 @@ __device__ void adj_col_edge(const AdjArgs<real>& a, const TeamFFT<real, N, E>& 
                     const cplx<real> P = cscale(cadd(a.wstate[idx], cconj(a.wstate[(size_t)jm * NXH + i])), (real)0.5);
                     lossg = cscale(P, a.loss_w * n4);
                 }
-                const bool keep = adj_keep(a, i, j);
                 cplx<real> cb[3] = {cscale(cw[e], sc), cscale(c1[e], sc), cscale(c2[e], sc)};
                 real Ef[3], Eh[3];
                 AdjHeld<real> held[3];
@@ -266,7 +266,7 @@ __device__ void adj_col_edge(const AdjArgs<real>& a, const TeamFFT<real, N, E>& 
                 }
 #pragma unroll
                 for (int f = 0; f < 3; ++f) {
-                    const cplx<real> kb = adj_rk_apply(a, f, idx, held[f], cb[f], Ef[f], Eh[f], keep,
+                    const cplx<real> kb = adj_rk_apply(a, f, idx, held[f], cb[f], Ef[f], Eh[f], adj_keep(a, f, i, j),
                                                        f == 0 ? lossg : mk<real>(0, 0));
                     a.edge[(size_t)(f * 2 + c) * N + j] = kb;
                 }
@@ -352,15 +352,14 @@ __global__ void __launch_bounds__(W * (N / E)) adj_col_kernel(const __grid_const
         for (int e = 0; e < E; ++e) {
             const int j = t + TEAM * e;
             const size_t idx = (size_t)j * NXH + i;
-            const bool keep = adj_keep(a, i, j);
             const cplx<real> lossg = a.wstate ? cscale(a.wstate[idx], 2 * a.loss_w * n4) : mk<real>(0, 0);
             real Ef0, Eh0, Ef, Eh;
             adj_factors<real, N>(a, 0, i, j, Ef0, Eh0);
             adj_factors<real, N>(a, 1, i, j, Ef, Eh);
             const AdjHeld<real> h0 = adj_rk_load(a, 0, idx), h1 = adj_rk_load(a, 1, idx), h2 = adj_rk_load(a, 2, idx);
-            cw[e] = adj_rk_apply(a, 0, idx, h0, cscale(cw[e], sc), Ef0, Eh0, keep, lossg);
-            c1[e] = adj_rk_apply(a, 1, idx, h1, cscale(c1[e], sc), Ef, Eh, keep, mk<real>(0, 0));
-            c2[e] = adj_rk_apply(a, 2, idx, h2, cscale(c2[e], sc), Ef, Eh, keep, mk<real>(0, 0));
+            cw[e] = adj_rk_apply(a, 0, idx, h0, cscale(cw[e], sc), Ef0, Eh0, adj_keep(a, 0, i, j), lossg);
+            c1[e] = adj_rk_apply(a, 1, idx, h1, cscale(c1[e], sc), Ef, Eh, adj_keep(a, 1, i, j), mk<real>(0, 0));
+            c2[e] = adj_rk_apply(a, 2, idx, h2, cscale(c2[e], sc), Ef, Eh, adj_keep(a, 2, i, j), mk<real>(0, 0));
         }
     }
     if (!a.emit) return;
@@ -439,7 +438,6 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
 #pragma unroll
                 for (int p = 0; p < PF_COUNT; ++p) cb[adj_target(p)] = cadd(cb[adj_target(p)], sm[(size_t)p * SPAN + j * W + w2]);
             const size_t idx = (size_t)j * NXH + i2;
-            const bool keep = adj_keep(a, i2, j);
             const cplx<real> lossg = wst ? cscale(wst[idx], 2 * lw * n2 * n2) : mk<real>(0, 0);
             real Ef[3], Eh[3];
             AdjHeld<real> held[3];
@@ -451,7 +449,8 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
 #pragma unroll
             for (int g = 0; g < 3; ++g)
                 sm[(size_t)g * SPAN + j * W + w2] = adj_rk_apply(a, g, so + idx, held[g], cscale(cb[g], 2 * n2), Ef[g],
-                                                                 Eh[g], keep, g == 0 ? lossg : mk<real>(0, 0));
+                                                                 Eh[g], adj_keep(a, g, i2, j),
+                                                                 g == 0 ? lossg : mk<real>(0, 0));
         }
         __syncthreads();
         if (!a.emit) return;
@@ -515,7 +514,6 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
             const cplx<real> P = cscale(cadd(wst[idx], cconj(wst[(size_t)jm * NXH + i])), (real)0.5);
             lossg = cscale(P, lw * n2 * n2);
         }
-        const bool keep = adj_keep(a, i, j);
         real Ef[3], Eh[3];
         AdjHeld<real> held[3];
 #pragma unroll
@@ -525,8 +523,8 @@ __global__ void __launch_bounds__(NGA * W * (N / E)) adj_colp_kernel(const __gri
         }
 #pragma unroll
         for (int g = 0; g < 3; ++g)
-            sm[(size_t)g * SPAN + c * N + j] = adj_rk_apply(a, g, so + idx, held[g], cscale(cb[g], n2), Ef[g], Eh[g], keep,
-                                                            g == 0 ? lossg : mk<real>(0, 0));
+            sm[(size_t)g * SPAN + c * N + j] = adj_rk_apply(a, g, so + idx, held[g], cscale(cb[g], n2), Ef[g], Eh[g],
+                                                            adj_keep(a, g, i, j), g == 0 ? lossg : mk<real>(0, 0));
     }
     __syncthreads();
     if (!a.emit) return;

@@ -269,16 +269,14 @@ qaf_status ensure_if(qaf_mesh* m, const qaf_params* p, cudaStream_t st) {
     return QAF_OK;
 }
 
-// the step's truncation of the new state: the 2/3 mask (dealias after stage 4,
-// friction.cu:253-255; keep i <= kx_keep && (j <= ky_lo || j >= ky_hi)), or a
-// mask that keeps every mode (the coupled runs, couple.cu:179-215, never dealias)
+// the step's truncation of the new state by the 2/3 mask (keep i <= kx_keep
+// && (j <= ky_lo || j >= ky_hi)) after stage 4, per field: all three
+// (no_dealias 0, friction.cu:253-255), none (1, the coupled runs,
+// couple.cu:179-215) or w only (2, dealias/couple.cu:226-229)
 template <class Args>
 void set_mask(Args& a, int N, int no_dealias) {
-    if (no_dealias) {
-        a.kx_keep = N / 2; a.ky_lo = N; a.ky_hi = N;
-    } else {
-        a.kx_keep = (N / 2) * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
-    }
+    a.kx_keep = (N / 2) * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
+    a.trunc = no_dealias == 0 ? 7 : (no_dealias == 2 ? 1 : 0);
 }
 
 template <typename real>
@@ -781,6 +779,7 @@ qaf_status qaf_integrate(qaf_mesh* m, qaf_integrator integ, int stage, const voi
 static qaf_status check_params(const qaf_params* p) {
     if (!p) return fail(QAF_ERR_INVALID, "null params");
     if (!(p->re > 0) || !(p->er > 0)) return fail(QAF_ERR_INVALID, "re and er must be positive");
+    if (p->no_dealias < 0 || p->no_dealias > 2) return fail(QAF_ERR_INVALID, "no_dealias must be 0, 1 or 2");
     if (!std::isfinite(p->dt) || !std::isfinite(p->lambda) || !std::isfinite(p->rf) || !std::isfinite(p->alpha) ||
         !std::isfinite(p->q_lin))
         return fail(QAF_ERR_INVALID, "non-finite parameter");

@@ -235,7 +235,7 @@ struct ColKernel {
                     const real Eh = Ehs[c];
                     const cplx<real> o = need_old ? ob[li] : mk<real>(0, 0);
                     const cplx<real> ac = need_acc ? ab[li] : mk<real>(0, 0);
-                    StageUpdate<real> u = stage_update(a, nl[e], o, ac, Ef, Eh, mask_keep(a, i, j));
+                    StageUpdate<real> u = stage_update(a, nl[e], o, ac, Ef, Eh, mask_keep(a, f, i, j));
                     if (!edge_col) {
                         if (u.write_acc) am[li] = u.acc;
                         if (u.write_old) {
@@ -482,7 +482,7 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int in
                     {
                         const size_t idx = (size_t)j * TW;
                         const real Ef = x0f * eyf[c], Eh = x0h * eyh[c];
-                        StageUpdate<real> u = stage_update(a, ctab[j], o0[c], a0[c], Ef, Eh, mask_keep(a, 0, j));
+                        StageUpdate<real> u = stage_update(a, ctab[j], o0[c], a0[c], Ef, Eh, mask_keep(a, f, 0, j));
                         if (u.write_acc) am[idx] = u.acc;
                         if (u.write_old) {
                             om[idx] = u.acc;
@@ -493,7 +493,7 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int in
                     // column kx = N/2
                     {
                         const real Ef = xHf * eyf[c], Eh = xHh * eyh[c];
-                        StageUpdate<real> u = stage_update(a, ctab[N + j], oH[c], aH[c], Ef, Eh, mask_keep(a, H, j));
+                        StageUpdate<real> u = stage_update(a, ctab[N + j], oH[c], aH[c], Ef, Eh, mask_keep(a, f, H, j));
                         if (u.write_acc) an[j] = u.acc;
                         if (u.write_old) {
                             on[j] = u.acc;

@@ -74,6 +74,7 @@ struct alignas(64) StageArgs {
     real dt;
     int advect;            // 1: keep -div(u w) in N_w
     int kx_keep, ky_lo, ky_hi;  // 2/3 mask: keep i <= kx_keep && (j <= ky_lo || j >= ky_hi)
+    int trunc;                  // fields the mask truncates after the last stage: bit f for field f
     // spectral state (internal layout)
     cplx<real>* old_m[3];
     cplx<real>* old_n[3];
@@ -201,8 +202,8 @@ __device__ __forceinline__ StageUpdate<real> stage_update(const StageArgs<real>&
 }
 
 template <typename real>
-__device__ __forceinline__ bool mask_keep(const StageArgs<real>& a, int i, int j) {
-    return i <= a.kx_keep && (j <= a.ky_lo || j >= a.ky_hi);
+__device__ __forceinline__ bool mask_keep(const StageArgs<real>& a, int f, int i, int j) {
+    return !((a.trunc >> f) & 1) || (i <= a.kx_keep && (j <= a.ky_lo || j >= a.ky_hi));
 }
 
 // Multiplier (times 1/N^2) that turns the spectral field f into the derived

@@ -78,7 +78,7 @@ class Params:
     dt: float = 1e-3
     q_lin: float = 1.0
     advect_omega: int = 1
-    no_dealias: int = 0      # 1: no 2/3 truncation per step (the coupled runs of UnitTest/TimeIntegration)
+    no_dealias: int = 0      # 1: no 2/3 truncation per step (the coupled runs); 2: of w only (dealias/couple.cu)
     alpha_field: Optional[object] = field(default=None, repr=False)   # torch tensor (ny, nx) on the device
 
     def c(self) -> CParams:

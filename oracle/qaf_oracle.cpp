@@ -670,6 +670,13 @@ int oracle_vel(const oracle_params* p, const double* w, double* u, double* v) {
     return 0;
 }
 
+// whether the step truncates field f by the 2/3 mask: all three fields
+// (friction.cu:253-255), none (no_dealias 1, couple.cu:179-215) or w only
+// (no_dealias 2, dealias/couple.cu:226-229)
+static bool truncates(const oracle_params* p, int f) {
+    return p->no_dealias == 0 || (p->no_dealias == 2 && f == 0);
+}
+
 int oracle_dealias(const oracle_params* p, double* spec) {   // dealias (Qsolver.cuh:314-322)
     if (!valid(p)) return 1;
     Mesh m(p);
@@ -790,8 +797,10 @@ int oracle_step(const oracle_params* p, int integrator, const double* alpha_fiel
                     nw[f][k] = (old[f][k] + an) * (*E[f])[k];
                 }
         }
-        for (int f = 0; f < 3; ++f)       // dealias + SpecSet(old <- new)
-            for (size_t k = 0; k < ns; ++k) old[f][k] = c.p->no_dealias ? nw[f][k] : nw[f][k] * c.m.cutoff[k];
+        for (int f = 0; f < 3; ++f) {     // dealias + SpecSet(old <- new)
+            const bool tr = truncates(c.p, f);
+            for (size_t k = 0; k < ns; ++k) old[f][k] = tr ? nw[f][k] * c.m.cutoff[k] : nw[f][k];
+        }
     }
     return 0;
 }
@@ -919,7 +928,7 @@ int oracle_step_tlm(const oracle_params* p, const double* alpha_field, const dou
             }
         for (int f = 0; f < 3; ++f)
             for (size_t k = 0; k < ns; ++k) {
-                const double keep = c.p->no_dealias ? 1.0 : c.m.cutoff[k];
+                const double keep = truncates(c.p, f) ? c.m.cutoff[k] : 1.0;
                 old[f][k] = nw[f][k] * keep;
                 dold[f][k] = dnw[f][k] * keep;
             }

@@ -40,7 +40,8 @@ typedef struct {
     double q_lin;          /* L_Q = -k^2 + q_lin (1.0 in the friction solver) */
     int advect_omega;      /* 1: keep -div(u w) in N_w (friction); 0: drop it */
     int emulate_symmetry;  /* 1: BwdTrans symmetrises its input's kx=0 column in place */
-    int no_dealias;        /* 1: steps skip the 2/3 truncation (couple.cu:179-215) */
+    int no_dealias;        /* 1: steps skip the 2/3 truncation (couple.cu:179-215); 2: truncate w only
+                              (dealias/couple.cu:226-229) */
 } oracle_params;
 
 enum { ORACLE_IFE = 0, ORACLE_IFRK2 = 1, ORACLE_IFRK4 = 2 };

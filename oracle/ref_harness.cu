@@ -65,7 +65,8 @@ struct Opts {
     uint64_t seed = 0;
     std::string out = "ref";
     int warmup = 3, timed = 10;
-    int dealias = 1;   // 0: the coupled runs' step, no truncation (couple.cu:179-215)
+    int dealias = 1;   // 0: the coupled runs' step, no truncation (couple.cu:179-215);
+                       // 2: dealias/couple.cu:226-229's, wnew truncated (three times) and r1, r2 not
 };
 
 void die(const char* msg) { std::fprintf(stderr, "ref_harness: %s\n", msg); std::exit(2); }
@@ -222,10 +223,12 @@ struct Solver {
         integrate_func4D<<<g, b>>>(wold->spec, wcurr->spec, wnew->spec, wnonl->spec, IFw, IFwh, Nxh, Ny, BSZ, dt);
         integrate_func4D<<<g, b>>>(r1old->spec, r1curr->spec, r1new->spec, r1nonl->spec, IFr1, IFr1h, Nxh, Ny, BSZ, dt);
         integrate_func4D<<<g, b>>>(r2old->spec, r2curr->spec, r2new->spec, r2nonl->spec, IFr2, IFr2h, Nxh, Ny, BSZ, dt);
-        if (do_dealias) {
+        if (do_dealias == 1) {
             dealias<<<g, b>>>(wnew->spec, mesh->cutoff, Nxh, Ny, BSZ);
             dealias<<<g, b>>>(r1new->spec, mesh->cutoff, Nxh, Ny, BSZ);
             dealias<<<g, b>>>(r2new->spec, mesh->cutoff, Nxh, Ny, BSZ);
+        } else if (do_dealias == 2) {
+            for (int k = 0; k < 3; ++k) dealias<<<g, b>>>(wnew->spec, mesh->cutoff, Nxh, Ny, BSZ);
         }
         SpecSet<<<g, b>>>(wold->spec, wnew->spec, Nxh, Ny, BSZ);
         SpecSet<<<g, b>>>(r1old->spec, r1new->spec, Nxh, Ny, BSZ);

@@ -19,6 +19,9 @@ noted; seeded random Q ~ U(-0.01, 0.01), w = 0, generator include/qaf_init.h):
                          0.1, Ra = 0.2, dt = 1e-3) from their smooth initial
                          state (qaf_couple_init, seed 9) on 64^2, L = 8 pi
                          (their grid spacing), states at steps 0 1 10 1000
+  dealiasw64             the same with the step of dealias/couple.cu:226-229
+                         (wnew truncated, r1 and r2 not), seed 11, states at
+                         steps 0 1 10 200
   kat summary            the reference's nonlinear terms for the analytic input
                          sets of UnitTest/Nonlinear/nlterms0-4 (N = 128, L = 2 pi,
                          Re = Er = 0.1, Ra = 0.2), reduced to their deviation from
@@ -43,8 +46,9 @@ import oracle as O  # noqa: E402
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 TWO_PI = "6.283185307179586"
 EIGHT_PI = "25.132741228718345"
-GROUPS = ("nl", "run32", "run64", "run128", "kat", "couple64")
+GROUPS = ("nl", "run32", "run64", "run128", "kat", "couple64", "dealiasw64")
 COUPLE_STEPS = (0, 1, 10, 1000)
+DEALIASW_STEPS = (0, 1, 10, 200)
 
 
 def run_harness(out, only=GROUPS):
@@ -64,6 +68,10 @@ def run_harness(out, only=GROUPS):
                       "--er", "0.1", "--rf", "0.000075", "--lambda", "0.1", "--alpha", "0.2", "--dt", "0.001",
                       "--dealias", "0", "--steps", str(COUPLE_STEPS[-1]),
                       "--dumps", ",".join(str(s) for s in COUPLE_STEPS), "--out", f"{out}/couple64"]],
+        "dealiasw64": [[H, "run", "--n", "64", "--L", EIGHT_PI, "--init", "couple", "--seed", "11", "--re", "0.1",
+                        "--er", "0.1", "--rf", "0.000075", "--lambda", "0.1", "--alpha", "0.2", "--dt", "0.001",
+                        "--dealias", "2", "--steps", str(DEALIASW_STEPS[-1]),
+                        "--dumps", ",".join(str(s) for s in DEALIASW_STEPS), "--out", f"{out}/dealiasw64"]],
     }
     for name in only:
         for c in jobs[name]:
@@ -127,6 +135,8 @@ def convert(d, only=GROUPS):
         save("ref_run128_s1000.npz", w=st[0], r1=st[1], r2=st[2])
     if "couple64" in only:
         save("ref_couple64.npz", **states("couple64", COUPLE_STEPS))
+    if "dealiasw64" in only:
+        save("ref_dealiasw64.npz", **states("dealiasw64", DEALIASW_STEPS))
     if "kat" not in only:
         return
     summary = {}

@@ -65,7 +65,7 @@ def _tlm_dJ(p, s0, alpha, d, dal, gT, nsteps, window):
     return dL + (_dot(gT, dsT) if gT is not None else 0.0)
 
 
-@pytest.mark.parametrize("advect,no_dealias", [(1, 0), (0, 0), (1, 1)])
+@pytest.mark.parametrize("advect,no_dealias", [(1, 0), (0, 0), (1, 1), (1, 2)])
 def test_gradient_matches_oracle_tlm_fp64(cuda, advect, no_dealias):
     import qaf
     n, T, K, Wn, dt = 32, 12, 5, 4, 1e-2

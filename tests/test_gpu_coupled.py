@@ -4,7 +4,8 @@ parameters (couple.cu:81-88: Re = Er = 0.1, Rf = 7.5e-5, lambda = 0.1,
 Ra = 0.2, dt = 1e-3) and the smooth initial state (couple.cu:4-35).
 
 Parity: the fused path against the reference's own build of that step
-(golden ref_couple64.npz) and against the FP64 oracle; the lowered linear
+(golden ref_couple64.npz) and against the FP64 oracle; the dealias/ variant
+(w truncated, r1 and r2 not, golden ref_dealiasw64.npz); the lowered linear
 coefficient of less/ (L_Q = -k^2 + 0.995, less/Qsolver.cuh:38,50) against the
 oracle. Long run: the observation recorded in couple/remark — over 40 time
 units on 512^2 (L = 66 pi) the scalar order S = 2 |(r1, r2)| stays near 1
@@ -56,6 +57,22 @@ def test_no_dealias_matches_reference_build_64(cuda):
     # the modes outside the 2/3 mask stay populated: the step really skipped the truncation
     cut = O.tables(O.params(n=64, L=8 * math.pi))[3]
     assert np.abs(host(st[1]) * (1 - cut)).max() > 0
+
+
+def test_w_only_truncation_matches_reference_build_64(cuda):
+    # dealias/couple.cu:226-229: wnew truncated by the 2/3 mask, r1 and r2 not
+    g = golden("ref_dealiasw64.npz")
+    m = qaf.Mesh(64, lx=8 * math.pi, dtype=qaf.F64)
+    st = [dev(g[f"{k}_0"], m) for k in ("w", "r1", "r2")]
+    prev = 0
+    for s, bar in ((1, 1e-13), (10, 1e-12), (200, 1e-11)):
+        m.step(couple_params(no_dealias=2), *st, nsteps=s - prev)
+        prev = s
+        for t, k in zip(st, ("w", "r1", "r2")):
+            assert O.rel_l2(host(t), g[f"{k}_{s}"]) < bar, (s, k)
+    cut = O.tables(O.params(n=64, L=8 * math.pi))[3]
+    assert np.abs(host(st[0]) * (1 - cut)).max() == 0          # w truncated
+    assert np.abs(host(st[1]) * (1 - cut)).max() > 0           # r1 not
 
 
 @pytest.mark.parametrize("dtype,steps,bar", [(qaf.F64, 20, 1e-12), (qaf.F32, 100, 1e-4)])

@@ -240,3 +240,26 @@ def test_coupled_step_matches_reference_build_64():
             assert O.rel_l2(a, g[f"{name}_{s}"]) < 1e-14, (s, name)
     w0, r10, r20 = (O.fwd(a) for a in O.couple_init(9, 64, 8 * np.pi))
     assert O.rel_l2(O.hermitian_part(r10), O.hermitian_part(g["r1_0"])) < 1e-15
+
+
+def test_w_only_truncation_step():
+    # dealias/couple.cu:226-229 truncates wnew only: one step gives the friction
+    # step's w and the coupled step's r1, r2
+    s0 = O.initial_spectra(1, 32)
+    full = O.step(O.params(n=32), *s0, 1)
+    none = O.step(O.params(n=32, no_dealias=1), *s0, 1)
+    w_only = O.step(O.params(n=32, no_dealias=2), *s0, 1)
+    assert np.array_equal(w_only[0], full[0])
+    assert np.array_equal(w_only[1], none[1]) and np.array_equal(w_only[2], none[2])
+
+
+def test_w_only_truncation_matches_reference_build_64():
+    g = golden("ref_dealiasw64.npz")
+    p = O.params(n=64, L=8 * np.pi, no_dealias=2, **COUPLE)
+    st = (g["w_0"], g["r1_0"], g["r2_0"])
+    prev = 0
+    for s in (1, 10):
+        st = O.step(p, *st, s - prev)
+        prev = s
+        for a, name in zip(st, ("w", "r1", "r2")):
+            assert O.rel_l2(a, g[f"{name}_{s}"]) < 1e-14, (s, name)
