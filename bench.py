@@ -102,6 +102,8 @@ def parse():
                     help="adjoint workload: launch shapes to use instead of tuning, e.g. col:e8m4,row:e8r2 "
                          "(to profile the shapes a tuned run reported)")
     ap.add_argument("--instances", type=int, default=ENS_COUNT)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="plain workload: skip the shortened FP64, adjoint and ensemble measurements")
     return ap.parse_args()
 
 
@@ -209,6 +211,29 @@ def barrier(world):
     torch.cuda.synchronize()
 
 
+def plain_config(n, world):
+    """The plain workload's config, the same dict in both arms."""
+    return {"workload": f"plain throughput {n}x{n}, L=16pi, IF-RK4 dt={DT}, Re=1 Rf=0.1 Er=1 lambda=0.1 Ra=1",
+            "grid": n, "integrator": "IF-RK4", "dt": DT, "seed": SEED, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 between timed steps (qaf: a 256 MiB write flushes it; the reference's "
+                  "22-field working set, ~185 MB in FP32, exceeds it)"}
+
+
+def traffic_of(kernel):
+    """Per-launch DRAM bytes (read + write) of `kernel` from profiles/traffic.txt
+    (ncu captures of the current kernels) and the commit they were captured at."""
+    tpath = os.path.join(ROOT, "profiles", "traffic.txt")
+    traffic, commit = None, None
+    if os.path.exists(tpath):
+        for line in open(tpath):
+            f = line.split()
+            if line.startswith("# captured at"):
+                commit = f[-1]
+            elif len(f) == 2 and not line.startswith("#") and f[0] == kernel:
+                traffic = float(f[1])
+    return traffic, commit
+
+
 def cpu_baseline(n, steps, dtype_name):
     """The FP64 host oracle (a restatement of the reference's scheme) on the
     host cores, on a bounded sample of the same workload."""
@@ -289,13 +314,7 @@ def run_qaf(a, world, rank, local):
     k_ms, k_bytes = kern[dom]
     peak, peak_kind = peaks()
     achieved = k_bytes / (k_ms * 1e-3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.txt")   # per-launch DRAM bytes from ncu captures
-    if os.path.exists(tpath):
-        for line in open(tpath):
-            f = line.split()
-            if len(f) == 2 and not line.startswith("#") and f[0] == f"{dom}_{a.dtype}_{n}":
-                traffic = float(f[1])
+    traffic, traffic_commit = traffic_of(f"{dom}_{a.dtype}_{n}")
 
     # ---- end to end through the public API, host I/O every step ----------
     # Step k's activity field is uploaded from pinned host memory on a copy
@@ -331,7 +350,7 @@ def run_qaf(a, world, rank, local):
             if k + 1 < steps:
                 flush.zero_()
 
-    e2e_steps = max(10, a.steps // 2)
+    e2e_steps = max(50, a.steps)
     diag_host = torch.empty((e2e_steps, 2), dtype=torch.float64).pin_memory()
     e2e_steps_run(2, diag_host)                    # warm-up of the same pipeline
     torch.cuda.synchronize()
@@ -347,17 +366,19 @@ def run_qaf(a, world, rank, local):
     assert bool(torch.isfinite(diag_host).all()) and bool((diag_host[:, 1] > 0).all())
     ms2 = max_over_ranks(t0.elapsed_time(t1), world)
     e2e = {"value": world * n * n * e2e_steps / (ms2 * 1e-3), "unit": UNIT,
-           "h2d_bytes_per_step": n * n * real_b, "d2h_bytes_per_step": 2 * 8}
+           "h2d_bytes_per_step": n * n * real_b, "d2h_bytes_per_step": 2 * 8, "steps": e2e_steps,
+           "what": "closed loop through the public API: the state stays resident; every step uploads the "
+                   "activity field from pinned host memory and reads back energy and enstrophy"}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": a.dtype, "data": "synthetic (seeded random Q ~ U(-0.01,0.01), w = 0)",
-        "config": {"workload": f"plain throughput {n}x{n}, L=16pi, IF-RK4 dt={DT}, Re=1 Rf=0.1 Er=1 lambda=0.1 Ra=1",
-                   "grid": n, "integrator": "IF-RK4", "dt": DT, "seed": SEED, "parallelism": f"replicas x{world}",
-                   "l2": "flushed (256 MiB write) between timed steps"},
+        "config": plain_config(n, world),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                        f"captured at commit {traffic_commit}" if traffic is not None else None),
                      "algorithmic_bytes_per_launch": k_bytes, "ms_per_launch": k_ms,
                      "row_ms": row_ms, "col_ms": col_ms},
         "e2e": e2e,
@@ -367,7 +388,121 @@ def run_qaf(a, world, rank, local):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"], oracle_run = cpu_baseline(n, a.cpu_sample_steps, a.dtype)
         line["spectrum_vs_oracle"] = spectrum_vs_oracle(mesh, qaf, oracle_run, a.cpu_sample_steps)
+    if world == 1 and not a.no_extras:
+        del mesh
+        line["targets"] = target_extras(a, qaf, torch, flush)
     return line
+
+
+def target_extras(a, qaf, torch, flush):
+    """Shortened measurements of the other stated targets, beside the headline:
+    the same workload in FP64, the adjoint's cost against a forward step (with
+    a finite-difference check of its gradient), and the batched ensemble
+    against the plain solver looped over the same instances."""
+    out = {}
+    # ---- the plain workload in FP64 (the reference's own precision) -------
+    if a.dtype != "f64":
+        m = qaf.Mesh(a.n, lx=L, dtype=qaf.F64)
+        p = qaf.Params(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=DT)
+        m.load(*m.random_q(SEED))
+        for _ in range(3):
+            m.advance(p, 1)
+        steps = 50
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record()
+            m.advance(p, 1)
+            e1.record()
+        torch.cuda.synchronize()
+        m.check_finite()
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+        out["fp64"] = {"value": a.n * a.n * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
+                       "steps": steps, "what": "the same workload in FP64, device resident, L2 flushed between steps"}
+        del m
+    # ---- adjoint cost (target: at most 3x a forward) ----------------------
+    T = 320
+    r = adjoint_ratio(qaf, torch, T, fd_dirs=4)
+    out["adjoint_cost_ratio"] = r
+    # ---- batched ensemble against the looped plain solver (target: >= 2x) -
+    out["ensemble_vs_looped"] = ensemble_ratio(qaf, torch, flush, steps=5)
+    return out
+
+
+def adjoint_ratio(qaf, torch, T, fd_dirs):
+    """The adjoint workload shortened to T steps: (recompute + adjoint) time
+    over the plain forward's, built-in launch shapes, plus the FD check."""
+    import numpy as np
+    n, dt = ADJ_N, ADJ_DT
+    K, Wn = min(ADJ_K, T), min(ADJ_WINDOW, T)
+    alpha_np = smoothed_alpha(n, ADJ_SEED)
+    base = dict(re=1.0, er=1.0, rf=0.1, lam=0.1, alpha=1.0, dt=dt, q_lin=1.0, advect_omega=1)
+    mesh = qaf.Mesh(n, lx=L, dtype=qaf.F32)
+    p = qaf.Params(**base)
+    p.alpha_field = torch.as_tensor(alpha_np).to(device="cuda", dtype=mesh.real_dtype)
+    s0 = mesh.random_q(SEED)
+    adj = qaf.Adjoint(mesh, T, K, Wn)
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    for _ in range(2):
+        mesh.load(*s0); mesh.advance(p, T)
+        adj.forward(p, *s0, final_state=False); adj.backward(None, 1.0)
+    tp, tb = [], []
+    for _ in range(3):
+        e0, e1 = ev()
+        mesh.load(*s0)
+        e0.record(); mesh.advance(p, T); e1.record()
+        torch.cuda.synchronize()
+        tp.append(e0.elapsed_time(e1))
+        adj.forward(p, *s0, final_state=False)
+        e0, e1 = ev()
+        e0.record(); adj.backward(None, 1.0); e1.record()
+        torch.cuda.synchronize()
+        tb.append(e0.elapsed_time(e1))
+    fwd, bwd = statistics.median(tp), statistics.median(tb)
+    fd = adjoint_fd_check(qaf, torch, np, n, T, K, Wn, dt, base, alpha_np, adj, p, s0, dirs=fd_dirs)
+    return {"value": bwd / fwd, "unit": "x", "forward_ms": fwd, "backward_ms": bwd, "fd_check": fd,
+            "what": f"{n}^2 FP32, {T} IF-RK4 steps dt={dt}, checkpoints every {K}, loss = mean enstrophy of the "
+                    f"last {Wn} states; (recompute + adjoint) / plain forward, medians of 3; built-in launch shapes"}
+
+
+def ensemble_ratio(qaf, torch, flush, steps):
+    """The 256-instance ensemble shortened to a few steps: the batched stepper
+    against the plain solver looped over the same instances (built-in shapes)."""
+    n_all, al, rf, seeds = ensemble_table(ENS_COUNT)
+    p = qaf.Params(re=1.0, er=1.0, rf=0.0, lam=0.1, alpha=1.0, dt=ENS_DT, q_lin=1.0, advect_omega=1)
+    ens = qaf.Ensemble(n_all, p, al, rf, lx=L, dtype=qaf.F32, tune=False)
+    ens.init_random(seeds)
+    for _ in range(2):
+        ens.advance(1)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(); ens.advance(1); e1.record()
+    torch.cuda.synchronize()
+    ens.diagnostics()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
+    del ens
+    states = []
+    for k in range(len(n_all)):
+        m = qaf.Mesh(n_all[k], lx=L, dtype=qaf.F32)
+        m.load(*m.random_q(seeds[k]))
+        states.append((m, qaf.Params(re=1.0, er=1.0, rf=rf[k], lam=0.1, alpha=al[k], dt=ENS_DT)))
+    for m, pk in states:
+        m.advance(pk, 1)
+    loop_steps = 3
+    flush.zero_()
+    l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0.record()
+    for m, pk in states:
+        m.advance(pk, loop_steps)
+    l1.record()
+    torch.cuda.synchronize()
+    ms_loop = l0.elapsed_time(l1) / loop_steps
+    work = sum(n * n for n in n_all)
+    return {"value": ms_loop / ms, "unit": "x", "batched_ms_per_step": ms, "looped_ms_per_step": ms_loop,
+            "batched": work / (ms * 1e-3), "looped": work / (ms_loop * 1e-3), "metric_unit": UNIT,
+            "what": f"{ens_workload_desc(ENS_COUNT)}; {steps} batched steps (one CUDA graph each) against "
+                    f"{loop_steps} steps of each instance through the plain solver; built-in launch shapes"}
 
 
 def run_reference(a, world, rank, local):
@@ -375,24 +510,35 @@ def run_reference(a, world, rank, local):
     if not os.path.exists(exe):
         return {"impl": "reference", "unavailable": "the reference's CUDA build (oracle/_ref) was not built: "
                                                     "its sources were not present when build() ran"}
-    cmd = [exe, "time", "--n", str(a.n), "--L", repr(L), "--dt", repr(DT), "--seed", str(SEED),
-           "--re", "1", "--er", "1", "--rf", "0.1", "--lambda", "0.1", "--alpha", "1",
-           "--warmup", str(a.warmup), "--timed", str(a.steps)]
-    env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
-    with ClockSampler(local) as clk:
+    def timed(path):
+        cmd = [path, "time", "--n", str(a.n), "--L", repr(L), "--dt", repr(DT), "--seed", str(SEED),
+               "--re", "1", "--er", "1", "--rf", "0.1", "--lambda", "0.1", "--alpha", "1",
+               "--warmup", str(a.warmup), "--timed", str(a.steps)]
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
         r = subprocess.run(cmd, capture_output=True, text=True, env=env)
-    if r.returncode != 0:
-        return {"impl": "reference", "unavailable": f"reference build exited {r.returncode}: {r.stderr.strip()[-200:]}"}
-    out = json.loads(r.stdout.strip().splitlines()[-1])
-    ms = out["ms_per_step"]
+        if r.returncode != 0:
+            return None, f"reference build exited {r.returncode}: {r.stderr.strip()[-200:]}"
+        return json.loads(r.stdout.strip().splitlines()[-1])["ms_per_step"], None
+
+    with ClockSampler(local) as clk:
+        ms, err = timed(exe)
+    if err:
+        return {"impl": "reference", "unavailable": err}
     value = a.n * a.n / (ms * 1e-3)
+    targets = {}
+    exe64 = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if a.dtype == "f32" and os.path.exists(exe64):
+        ms64, err64 = timed(exe64)
+        targets["fp64"] = ({"value": a.n * a.n / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
+                            "steps": a.steps, "what": "the reference's build as shipped (FP64), same workload"}
+                           if err64 is None else {"unavailable": err64})
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": a.dtype, "data": "synthetic (seeded random Q ~ U(-0.01,0.01), w = 0)",
-        "config": {"workload": f"plain throughput {a.n}x{a.n}, L=16pi, IF-RK4 dt={DT}, Re=1 Rf=0.1 Er=1 lambda=0.1 Ra=1",
-                   "grid": a.n, "integrator": "IF-RK4", "dt": DT, "seed": SEED, "parallelism": "single GPU",
-                   "l2": "working set (22 fields, ~185 MB in FP32) larger than L2"},
+        "config": plain_config(a.n, world),
+        "targets": targets,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": f"{a.steps} steps of the reference's own CUDA build (friction.cu step sequence, "
                                    f"unmodified headers{', FP32 macro shim' if a.dtype == 'f32' else ''}) on the B200; "
@@ -710,9 +856,9 @@ def run_adjoint(a, world, rank, local):
     return line
 
 
-def adjoint_fd_check(qaf, torch, np, n, T, K, Wn, dt, base, alpha_np, adj32, p32, s0_32):
+def adjoint_fd_check(qaf, torch, np, n, T, K, Wn, dt, base, alpha_np, adj32, p32, s0_32, dirs=16):
     """Directional derivatives of the FP32 and FP64 adjoint gradients against central
-    differences of the FP64 forward, along 16 random directions of (Ra(x), initial spectra)."""
+    differences of the FP64 forward, along `dirs` random directions of (Ra(x), initial spectra)."""
     mesh = qaf.Mesh(n, lx=L, dtype=qaf.F64)
     p = qaf.Params(**base)
     alpha = torch.as_tensor(alpha_np, dtype=torch.float64, device="cuda")
@@ -726,7 +872,7 @@ def adjoint_fd_check(qaf, torch, np, n, T, K, Wn, dt, base, alpha_np, adj32, p32
     rng = np.random.default_rng(7)
     scale = float(max(x.abs().max().item() for x in s0[1:]))
     err32, err64 = [], []
-    for _ in range(16):
+    for _ in range(dirs):
         da = torch.as_tensor(smoothed_alpha(n, int(rng.integers(1 << 30))) - 1.0, device="cuda") * 10.0
         ds = [torch.complex(torch.as_tensor(rng.standard_normal(x.shape)), torch.as_tensor(rng.standard_normal(x.shape)))
               .to("cuda") * scale for x in s0]
@@ -747,7 +893,7 @@ def adjoint_fd_check(qaf, torch, np, n, T, K, Wn, dt, base, alpha_np, adj32, p32
             return v
         err64.append(abs(dot(g64) - fdv) / abs(fdv))
         err32.append(abs(dot(g32) - fdv) / abs(fdv))
-    return {"directions": 16, "eps": 1e-5, "loss": loss0,
+    return {"directions": dirs, "eps": 1e-5, "loss": loss0,
             "max_rel_err_fp64_adjoint": max(err64), "max_rel_err_fp32_adjoint": max(err32),
             "median_rel_err_fp32_adjoint": statistics.median(err32),
             "reference": "central differences of the FP64 forward on the GPU"}

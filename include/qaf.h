@@ -174,6 +174,16 @@ qaf_status qaf_state_advance_timed(qaf_mesh* mesh, const qaf_params* p, qaf_inte
                                    double out_ms[3], void* stream);
 /* Number of kernels this mesh has launched so far. */
 uint64_t qaf_launch_count(const qaf_mesh* mesh);
+/* Test hook for the bounded copy waits; no counterpart in the reference
+ * (whose only failure check is the NaN test, friction.cu:280). The next
+ * fused-step column launch of an RK stage in this process (not the launch
+ * that first transforms a loaded state) arms slab `slab` (>= 0) of the
+ * copy sequence of its queue item 0 but never issues that copy, and every
+ * copy wait of that launch gives up after `polls` (>= 1) tries. The CTA whose
+ * wait ran out stops at the next item boundary with no copy in flight, and
+ * the step reports QAF_ERR_CUDA through qaf_check_finite /
+ * qaf_last_diagnostics. One launch only: the hook clears itself. */
+qaf_status qaf_test_lose_copy(int slab, unsigned polls);
 
 /* ---- seeded initial state -------------------------------------------------
  * The reference reads its initial Q from CSV files or fills it with libc
@@ -293,9 +303,19 @@ qaf_status qaf_adjoint_batch_backward(qaf_adjoint_batch* batch, const void* gwT,
  * current; make that first call before any stream capture. All calls share the
  * one array: calls whose work overlaps on the GPU (other streams, other host
  * threads) race and must be serialised by the caller. The array keeps the last
- * call's contents; each call rebuilds what it needs. */
+ * call's contents; each call rebuilds what it needs. Its twiddles and
+ * integrating factors are built on the device (sincospi / exp in double),
+ * where qaf_step's come from long-double host tables, so the two agree to
+ * rounding (last bits), not bit for bit.
+ * The call returns once its work is queued on `stream`, so a kernel failure
+ * cannot be in its return value: `status` (NULL: not wanted) is a device or
+ * page-locked host word that receives, in stream order after the step, the
+ * call's status flags — 0 when all went well, bit 0 a non-finite value in the
+ * new state, bit 1 a bounded copy wait that gave up (the state is then not
+ * valid). Read it once the stream has reached that point. */
 qaf_status qaf_step_noalloc(int n, double lx, double ly, qaf_dtype dtype, const qaf_params* p,
-                            qaf_integrator integ, void* w, void* r1, void* r2, int nsteps, void* stream);
+                            qaf_integrator integ, void* w, void* r1, void* r2, int nsteps, void* status,
+                            void* stream);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,10 @@ def build(force=False, verbose=True, extra=()):
     if not force and not needs_build():
         return OUT
     nvcc = os.environ.get("NVCC", "nvcc")
+    # QAF_SPLIT_COMPILE=1: compile each file's kernels in parallel threads
+    # (shorter builds while iterating; timed builds use the default)
+    if os.environ.get("QAF_SPLIT_COMPILE") == "1":
+        extra = (*extra, "--split-compile=0")
     objs = []
     tmpdir = os.path.join(PKG, "_build")
     os.makedirs(tmpdir, exist_ok=True)

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -47,6 +48,50 @@ qaf_status fail(qaf_status st, const std::string& msg) {
     } while (0)
 
 bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// ---------------------------------------------------------------------------
+// One-time set-up per device. Kernel attributes (cudaFuncSetAttribute) and
+// occupancy apply to the device that is current when they are set, so every
+// set-up step keeps one slot per device index, filled under one lock the first
+// time a call runs on that device; later calls read it without the lock.
+// ---------------------------------------------------------------------------
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mu;
+
+qaf_status current_device(int* dev) {
+    QAF_CUDA(cudaGetDevice(dev));
+    if (*dev < 0 || *dev >= kMaxDevices) return fail(QAF_ERR_UNSUPPORTED, "device index out of range");
+    return QAF_OK;
+}
+
+struct DeviceOnce {
+    std::atomic<int> v[kMaxDevices] = {};   // 0: not set up on that device
+    // the value for the current device; init(int* value) runs once per device
+    // (value >= 1 once set up)
+    template <class F>
+    qaf_status get(int* out, F&& init) {
+        int dev = 0;
+        QAF_TRY(current_device(&dev));
+        int x = v[dev].load(std::memory_order_acquire);
+        if (x == 0) {
+            std::lock_guard<std::mutex> g(g_setup_mu);
+            x = v[dev].load(std::memory_order_relaxed);
+            if (x == 0) {
+                QAF_TRY(init(&x));
+                if (x < 1) x = 1;
+                v[dev].store(x, std::memory_order_release);
+            }
+        }
+        if (out) *out = x;
+        return QAF_OK;
+    }
+    // the value set up for the current device, 0 if none
+    int peek() const {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+        return v[dev].load(std::memory_order_acquire);
+    }
+};
 
 // Launch-shape defaults (values per thread of the column / row FFTs, threads
 // per row-kernel CTA); overridable at build time for tuning.
@@ -126,18 +171,20 @@ size_t align_up(size_t x) { return (x + 31) & ~size_t(31); }
 // TMA descriptor of the G arrays: [NG*N rows][H columns] of 8-byte elements
 // (two per FP64 complex), boxes of TW columns x min(N, 256) rows.
 template <typename real>
-qaf_status encode_g_map(CUtensorMap* tm, const cplx<real>* G, int N) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
+qaf_status encode_g_map(CUtensorMap* tm, const cplx<real>* G, int N, size_t rows = 0) {
+    // looked up once per process (a function-local static: thread-safe)
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
         cudaDriverEntryPointQueryResult q;
         void* fn = nullptr;
-        QAF_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-        if (q != cudaDriverEntryPointSuccess || !fn) return fail(QAF_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
+    if (!encode) return fail(QAF_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     const int H = N / 2;
     const cuuint64_t cpe = sizeof(cplx<real>) / 8;
-    cuuint64_t dims[2] = {(cuuint64_t)H * cpe, (cuuint64_t)NG * N};
+    cuuint64_t dims[2] = {(cuuint64_t)H * cpe, (cuuint64_t)(rows ? rows : (size_t)NG * N)};
     cuuint64_t strides[1] = {(cuuint64_t)H * cpe * 8};
     cuuint32_t box[2] = {(cuuint32_t)(TW * cpe), (cuuint32_t)(N < 256 ? N : 256)};
     cuuint32_t estr[2] = {1, 1};
@@ -282,7 +329,7 @@ void set_mask(Args& a, int N, int no_dealias) {
 template <typename real>
 StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
     Workspace<real>& w = ws<real>(m);
-    const int N = m->desc.nx, nxh = N / 2 + 1;
+    const int N = m->desc.nx;
     StageArgs<real> a;
     std::memset(&a, 0, sizeof(a));
     a.dkx = (real)m->dkx; a.dky = (real)m->dky;
@@ -318,31 +365,40 @@ int variant_list(int dtype, int n, StepVariant<float>** out) {
     return dtype == QAF_F32 ? step_variants_f32(n, out) : 0;
 }
 
-// the variant to launch for kind (0 column, 1 row), or nullptr for the built-in shape
-StepVariant<float>* tuned_variant(int n, int kind, bool batched) {
+// set-up of each variant per device: resident column CTAs (column variants)
+// or 1 (row variants, attributes only), keyed by (variant, device)
+std::map<std::pair<const StepVariant<float>*, int>, int> g_variant_setup;
+
+// the variant to launch for kind (0 column, 1 row), or nullptr for the
+// built-in shape; *slots receives its persistent grid size on this device
+StepVariant<float>* tuned_variant(int n, int kind, bool batched, int* slots) {
     int idx = -1;
-    {
-        std::lock_guard<std::mutex> lk(g_tune_mu);
-        if (g_tune.empty()) return nullptr;
-        auto it = g_tune.find(std::make_tuple((int)QAF_F32, n, batched ? 1 : 0));
-        if (it == g_tune.end()) return nullptr;
-        idx = kind == 0 ? it->second.col : it->second.row;
-    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (g_tune.empty()) return nullptr;
+    auto it = g_tune.find(std::make_tuple((int)QAF_F32, n, batched ? 1 : 0));
+    if (it == g_tune.end()) return nullptr;
+    idx = kind == 0 ? it->second.col : it->second.row;
     if (idx < 0) return nullptr;
     StepVariant<float>* v = nullptr;
     const int cnt = step_variants_f32(n, &v);
     if (idx >= cnt) return nullptr;
-    if (v[idx].slots == 0 && v[idx].kind == 0) {
-        int slots = 0;
-        if (v[idx].setup(&slots) != cudaSuccess || slots < 1) return nullptr;
-        v[idx].slots = slots;
-    } else if (v[idx].kind == 1 && v[idx].slots == 0) {
-        int unused = 0;
-        if (v[idx].setup(&unused) != cudaSuccess) return nullptr;
-        v[idx].slots = -1;   // set up
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    const auto key = std::make_pair((const StepVariant<float>*)&v[idx], dev);
+    auto s = g_variant_setup.find(key);
+    if (s == g_variant_setup.end()) {
+        int got = 0;
+        if (v[idx].setup(&got) != cudaSuccess) return nullptr;
+        if (v[idx].kind == 0 && got < 1) return nullptr;
+        s = g_variant_setup.emplace(key, v[idx].kind == 0 ? got : 1).first;
     }
+    *slots = s->second;
     return &v[idx];
 }
+
+// test hook of qaf_test_lose_copy: consumed by the next column launch
+std::atomic<int> g_test_drop{0};        // slab + 1, 0: off
+std::atomic<unsigned> g_test_polls{0};
 
 // ---------------------------------------------------------------------------
 // per-size launchers
@@ -350,39 +406,53 @@ StepVariant<float>* tuned_variant(int n, int kind, bool batched) {
 template <typename real, int N>
 struct Launch {
     using C = Cfg<real, N>;
-    static inline int col_slots = 0;    // resident column CTAs on the device (persistent grid size)
+    // resident column CTAs per device (the persistent grid size)
+    static inline DeviceOnce col_slots;
     static qaf_status setup() {
-        static bool done = false;
-        if (done) return QAF_OK;
-        QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::EC, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
-        QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::ROW_SMEM));
-        QAF_CUDA(cudaFuncSetAttribute(col_ifft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
-        QAF_CUDA(cudaFuncSetAttribute(col_fft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
-        int dev = 0, sms = 0, per_sm = 0;
-        QAF_CUDA(cudaGetDevice(&dev));
-        QAF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        QAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_kernel<real, N, C::EC, C::MINB>,
-                                                               C::COL_THREADS, C::COL_SMEM));
-        if (per_sm < 1) return fail(QAF_ERR_UNSUPPORTED, "column kernel does not fit on an SM");
-        col_slots = sms * per_sm;
-        done = true;
-        return QAF_OK;
+        return col_slots.get(nullptr, [](int* slots) -> qaf_status {
+            QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::EC, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
+            QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::ROW_SMEM));
+            QAF_CUDA(cudaFuncSetAttribute(col_ifft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
+            QAF_CUDA(cudaFuncSetAttribute(col_fft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
+            int dev = 0, sms = 0, per_sm = 0;
+            QAF_CUDA(cudaGetDevice(&dev));
+            QAF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            QAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_kernel<real, N, C::EC, C::MINB>,
+                                                                   C::COL_THREADS, C::COL_SMEM));
+            if (per_sm < 1) return fail(QAF_ERR_UNSUPPORTED, "column kernel does not fit on an SM");
+            *slots = sms * per_sm;
+            return QAF_OK;
+        });
     }
-    static void col(const StageArgs<real>& a, cudaStream_t st) {
+    static void col(const StageArgs<real>& a0, cudaStream_t st) {
+        StageArgs<real> hooked;
+        const StageArgs<real>* ap = &a0;
+        if (a0.mode == MODE_STAGE && g_test_drop.load(std::memory_order_relaxed) != 0) {
+            if (const int d = g_test_drop.exchange(0)) {
+                hooked = a0;
+                hooked.drop_slab = d;
+                hooked.wait_polls = g_test_polls.load();
+                ap = &hooked;
+            }
+        }
+        const StageArgs<real>& a = *ap;
         if constexpr (std::is_same<real, float>::value) {
-            if (StepVariant<float>* v = tuned_variant(N, 0, a.ninst > 1)) {
-                v->launch(a, v->slots, st);
+            int slots = 0;
+            if (StepVariant<float>* v = tuned_variant(N, 0, a.ninst > 1, &slots)) {
+                v->launch(a, slots, st);
                 return;
             }
         }
         const long items = (long)C::COL_ITEMS * a.ninst;
-        const int grid = items < col_slots ? (int)items : col_slots;
+        const int slots = col_slots.peek();   // set up by every operation before its launches
+        const int grid = slots > 0 && items > slots ? slots : (int)items;
         col_kernel<real, N, C::EC, C::MINB><<<grid, C::COL_THREADS, C::COL_SMEM, st>>>(a);
     }
     static void row(const StageArgs<real>& a, cudaStream_t st) {
         if constexpr (std::is_same<real, float>::value) {
-            if (StepVariant<float>* v = tuned_variant(N, 1, a.ninst > 1)) {
-                v->launch(a, v->slots, st);
+            int slots = 0;
+            if (StepVariant<float>* v = tuned_variant(N, 1, a.ninst > 1, &slots)) {
+                v->launch(a, slots, st);
                 return;
             }
         }
@@ -866,6 +936,13 @@ qaf_status qaf_state_advance_timed(qaf_mesh* m, const qaf_params* p, qaf_integra
 
 uint64_t qaf_launch_count(const qaf_mesh* m) { return m ? m->launches : 0; }
 
+qaf_status qaf_test_lose_copy(int slab, unsigned polls) {
+    if (slab < 0 || polls < 1) return fail(QAF_ERR_INVALID, "qaf_test_lose_copy: slab >= 0 and polls >= 1");
+    g_test_polls.store(polls);
+    g_test_drop.store(slab + 1);
+    return QAF_OK;
+}
+
 qaf_status qaf_step(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, void* w, void* r1, void* r2, int nsteps,
                     void* stream) {
     QAF_TRY(check_advance(m, p, integ, nsteps));
@@ -1082,7 +1159,6 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // Device address of g_noalloc_scratch per device, looked up once per device
 // (with that device current) on the first call made on it.
-constexpr int kMaxDevices = 64;
 unsigned char* g_noalloc_ptr[kMaxDevices] = {};
 std::mutex g_noalloc_mu;
 
@@ -1155,7 +1231,7 @@ __global__ void noalloc_tables_kernel(cplx<real>* tw, real* ex, real* ey, int N,
 struct OpStepNoAlloc {
     template <typename real, int N>
     static qaf_status run(qaf_mesh* m, unsigned char* scratch, const qaf_params* p, int integ, void* const* state,
-                          int nsteps, cudaStream_t st) {
+                          int nsteps, void* status, cudaStream_t st) {
         if (N > kNoAllocMaxN) return fail(QAF_ERR_INVALID, "qaf_step_noalloc: grid larger than 128 x 128");
         Workspace<real>& w = ws<real>(m);
         const size_t need = noalloc_carve<real>(w, reinterpret_cast<cplx<real>*>(scratch), N);
@@ -1194,14 +1270,19 @@ struct OpStepNoAlloc {
         }
         for (int f = 0; f < 3; ++f)
             from_internal<real>(m, w.old_m[f], w.old_n[f], state[f], st);
-        return post_launch("qaf_step_noalloc");
+        QAF_TRY(post_launch("qaf_step_noalloc"));
+        // the call's status flags, in stream order, for the caller to read
+        // once the stream has reached this point
+        if (status) QAF_CUDA(cudaMemcpyAsync(status, w.flags, sizeof(unsigned), cudaMemcpyDefault, st));
+        return QAF_OK;
     }
 };
 
 }  // namespace
 
 extern "C" qaf_status qaf_step_noalloc(int n, double lx, double ly, qaf_dtype dtype, const qaf_params* p,
-                                       qaf_integrator integ, void* w, void* r1, void* r2, int nsteps, void* stream) {
+                                       qaf_integrator integ, void* w, void* r1, void* r2, int nsteps, void* status,
+                                       void* stream) {
     if (!p || !w || !r1 || !r2) return fail(QAF_ERR_INVALID, "qaf_step_noalloc: null pointer");
     if (n < 16 || n > kNoAllocMaxN || (n & (n - 1)))
         return fail(QAF_ERR_INVALID, "qaf_step_noalloc: n must be a power of two in [16, 128] "
@@ -1211,7 +1292,10 @@ extern "C" qaf_status qaf_step_noalloc(int n, double lx, double ly, qaf_dtype dt
     QAF_TRY(check_params(p));
     if (integ != QAF_IFE && integ != QAF_IFRK2 && integ != QAF_IFRK4) return fail(QAF_ERR_INVALID, "bad integrator");
     if (nsteps < 0) return fail(QAF_ERR_INVALID, "nsteps < 0");
-    if (nsteps == 0) return QAF_OK;
+    if (nsteps == 0) {
+        if (status) QAF_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned), (cudaStream_t)stream));
+        return QAF_OK;
+    }
     unsigned char* scratch = nullptr;
     QAF_TRY(noalloc_scratch(&scratch));
     // a mesh description on the stack whose workspace points into the fixed array
@@ -1220,9 +1304,10 @@ extern "C" qaf_status qaf_step_noalloc(int n, double lx, double ly, qaf_dtype dt
     m.nxh = n / 2 + 1;
     m.dkx = 2 * M_PI / lx;
     m.dky = 2 * M_PI / ly;
-    m.device = 0;
+    QAF_CUDA(cudaGetDevice(&m.device));
     void* st[3] = {w, r1, r2};
-    return dispatch<OpStepNoAlloc>(&m, &m, scratch, p, (int)integ, (void* const*)st, nsteps, (cudaStream_t)stream);
+    return dispatch<OpStepNoAlloc>(&m, &m, scratch, p, (int)integ, (void* const*)st, nsteps, status,
+                                   (cudaStream_t)stream);
 }
 
 // ===========================================================================
@@ -1316,7 +1401,7 @@ template <typename real>
 StageArgs<real> group_args(const qaf_ensemble* e, const EnsGroup<real>& g) {
     StageArgs<real> a;
     std::memset(&a, 0, sizeof(a));
-    const int N = g.N, nxh = N / 2 + 1;
+    const int N = g.N;
     a.dkx = (real)(2 * M_PI / e->lx); a.dky = (real)(2 * M_PI / e->ly);
     a.lambda = (real)e->p.lambda; a.ce = (real)(1.0 / (e->p.er * e->p.re)); a.alpha = (real)e->p.alpha;
     a.dt = (real)e->p.dt; a.advect = e->p.advect_omega ? 1 : 0;
@@ -1390,25 +1475,7 @@ qaf_status build_groups(qaf_ensemble* e, const double* alpha, const double* rf) 
         QAF_CUDA(cudaMemset(g.w.flags, 0, 16));
         QAF_CUDA(cudaMemset(g.diag, 0, 2 * (size_t)g.ninst * sizeof(double)));
         // TMA view of every instance's G arrays
-        {
-            static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-            if (!encode) {
-                cudaDriverEntryPointQueryResult q;
-                void* fn = nullptr;
-                QAF_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-                if (q != cudaDriverEntryPointSuccess || !fn) return fail(QAF_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-                encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-            }
-            const cuuint64_t cpe = sizeof(cplx<real>) / 8;
-            cuuint64_t dims[2] = {(cuuint64_t)H * cpe, (cuuint64_t)(g.ninst - 1) * (g.istride / H) + (cuuint64_t)NG * N};
-            cuuint64_t strides[1] = {(cuuint64_t)H * cpe * 8};
-            cuuint32_t box[2] = {(cuuint32_t)(TW * cpe), (cuuint32_t)(N < 256 ? N : 256)};
-            cuuint32_t estr[2] = {1, 1};
-            CUresult r = encode(&g.w.tm_G, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, g.w.G, dims, strides, box, estr,
-                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-            if (r != CUDA_SUCCESS) return fail(QAF_ERR_CUDA, "cuTensorMapEncodeTiled failed (ensemble)");
-        }
+        QAF_TRY(encode_g_map<real>(&g.w.tm_G, g.w.G, N, (size_t)(g.ninst - 1) * (g.istride / H) + (size_t)NG * N));
         qaf_status st = with_n(N, [&](auto n) -> qaf_status { return Launch<real, decltype(n)::value>::setup(); });
         if (st != QAF_OK) return st;
         G.push_back(g);
@@ -1811,15 +1878,15 @@ struct OpAdjBackward {
         constexpr int ER = H / 16 < 2 ? 2 : (H / 16 > 16 ? 16 : H / 16);
         constexpr int ROW_THREADS = NGA * (H / ER);
         constexpr size_t ROW_SMEM = (size_t)NGA * H * sizeof(cplx<real>);
-        static bool attrs = false;
-        if (!attrs) {
+        static DeviceOnce attrs;   // kernel attributes, per device
+        QAF_TRY(attrs.get(nullptr, [](int*) -> qaf_status {
             if constexpr (FP)
                 QAF_CUDA(cudaFuncSetAttribute(adj_colp_kernel<real, N, W, EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COL_SMEM));
             else
                 QAF_CUDA(cudaFuncSetAttribute(adj_col_kernel<real, N, W, EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COL_SMEM));
             QAF_CUDA(cudaFuncSetAttribute(adj_row_kernel<real, N, ER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROW_SMEM));
-            attrs = true;
-        }
+            return QAF_OK;
+        }));
         qaf_mesh* m = A->m;
         const size_t ns = A->ns, cb = sizeof(cplx<real>);
         const size_t slot = (size_t)PF_COUNT * N * N;
@@ -2388,12 +2455,12 @@ qaf_status batch_backward(qaf_adjoint_batch* B, const void* const* gT, const dou
     constexpr int ER = H / 16 < 2 ? 2 : (H / 16 > 16 ? 16 : H / 16);
     constexpr int ROW_THREADS = NGA * (H / ER);
     constexpr size_t ROW_SMEM = (size_t)NGA * H * sizeof(cplx<real>);
-    static bool attrs = false;
-    if (!attrs) {
+    static DeviceOnce attrs;   // kernel attributes, per device
+    QAF_TRY(attrs.get(nullptr, [](int*) -> qaf_status {
         QAF_CUDA(cudaFuncSetAttribute(adj_colp_kernel<real, N, W, EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)COL_SMEM));
         QAF_CUDA(cudaFuncSetAttribute(adj_row_kernel<real, N, ER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROW_SMEM));
-        attrs = true;
-    }
+        return QAF_OK;
+    }));
     qaf_ensemble* e = B->ens;
     EnsGroup<real>& g = O::group(B);
     const size_t ns = B->ns, cb = sizeof(cplx<real>), ni = (size_t)B->ninst;

@@ -40,17 +40,24 @@ template <typename C> QAF_HD C cmul_mi(C a) { C c; c.x = a.y; c.y = -a.x; return
 // a * conj(w) when INV, a * w otherwise
 template <bool INV, typename C> QAF_HD C ctw(C a, C w) { if (INV) w.y = -w.y; return cmul(a, w); }
 
-// cos and sin of 2 pi k / 16, k = 0..15 (mathematical constants to double precision)
-QAF_HD double cos16(int k) {
-    const double c[16] = {1.0, 0.92387953251128673848, 0.70710678118654752440, 0.38268343236508977173,
-                          0.0, -0.38268343236508977173, -0.70710678118654752440, -0.92387953251128673848,
-                          -1.0, -0.92387953251128673848, -0.70710678118654752440, -0.38268343236508977173,
-                          0.0, 0.38268343236508977173, 0.70710678118654752440, 0.92387953251128673848};
-    return c[k & 15];
+// cos and sin of 2 pi k / 48 for any integer k (mathematical constants to
+// double precision; the first quadrant is tabulated, the rest by symmetry).
+// 48 = 3 * 16 covers every twiddle of the small DFTs below (R | 48).
+QAF_HD double cos48(int k) {
+    const double c[13] = {1.0, 0.99144486137381041114, 0.96592582628906828675, 0.92387953251128675613,
+                          0.86602540378443864676, 0.79335334029123516458, 0.70710678118654752440,
+                          0.60876142900872063942, 0.5, 0.38268343236508977173, 0.25881904510252076235,
+                          0.13052619222005159155, 0.0};
+    k = ((k % 48) + 48) % 48;
+    if (k <= 12) return c[k];
+    if (k <= 24) return -c[24 - k];
+    if (k <= 36) return -c[k - 24];
+    return c[48 - k];
 }
-QAF_HD double sin16(int k) { return cos16(k + 12); }   // sin(x) = cos(x - pi/2)
+QAF_HD double sin48(int k) { return cos48(k + 36); }   // sin x = cos(x - pi/2)
 
 QAF_HDC int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+QAF_HDC bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 // iterative (not recursive) so that, with constant arguments after unrolling,
 // the device compiler folds it and register arrays indexed by it stay in registers
 QAF_HDC int bitrev(int x, int bits) {
@@ -59,39 +66,81 @@ QAF_HDC int bitrev(int x, int bits) {
     return r;
 }
 
-// In-register DFT of R = 2, 4, 8 or 16 points: y[r] = sum_q x[q] W_R^{qr},
-// W_R = exp(-2 pi i / R) (forward) or exp(+2 pi i / R) (INV). Iterative
-// radix-2 on a bit-reversed copy; all indices are compile-time constants.
+// a * W_R^m with W_R = exp(-2 pi i / R) (forward) or exp(+2 pi i / R) (INV),
+// m a compile-time constant after unrolling, R | 48
+template <typename real, int R, bool INV>
+QAF_HD cplx<real> rot(cplx<real> a, int m) {
+    const int k = ((m % R) + R) % R * (48 / R);   // angle 2 pi k / 48
+    if (k == 0) return a;
+    if (k == 12) return INV ? cmul_i(a) : cmul_mi(a);
+    if (k == 24) return mk<real>(-a.x, -a.y);
+    if (k == 36) return INV ? cmul_mi(a) : cmul_i(a);
+    const cplx<real> w = mk<real>((real)cos48(k), (real)(INV ? sin48(k) : -sin48(k)));
+    return cmul(a, w);
+}
+
+// 3-point DFT in place: y_r = sum_q x_q W_3^{qr}
+template <typename real, bool INV>
+QAF_HD void dft3(cplx<real>& x0, cplx<real>& x1, cplx<real>& x2) {
+    const real h = (real)0.86602540378443864676;   // sin(2 pi / 3)
+    const cplx<real> t1 = cadd(x1, x2), t2 = csub(x1, x2);
+    const cplx<real> m = mk<real>(x0.x - (real)0.5 * t1.x, x0.y - (real)0.5 * t1.y);
+    // forward: y1 = m - i h t2, y2 = m + i h t2 (inverse: the signs swap)
+    const cplx<real> r = mk<real>(-h * t2.y, h * t2.x);    // i h t2
+    x0 = cadd(x0, t1);
+    x1 = INV ? cadd(m, r) : csub(m, r);
+    x2 = INV ? csub(m, r) : cadd(m, r);
+}
+
+// In-register DFT of R points, R = 2^m (m <= 4) or 3 * 2^m (m <= 4):
+// y[r] = sum_q x[q] W_R^{qr}, W_R = exp(-2 pi i / R) (forward) or
+// exp(+2 pi i / R) (INV). Powers of two: iterative radix-2 on a bit-reversed
+// copy. 3 * Q: Cooley-Tukey with n = Q n1 + n2, k = k1 + 3 k2 — three-point
+// DFTs over n1, twiddles W_R^{n2 k1}, then Q-point DFTs over n2. All indices
+// are compile-time constants.
 template <typename real, int R, bool INV>
 QAF_HD void small_dft(cplx<real>* x) {
-    static_assert(R == 1 || R == 2 || R == 4 || R == 8 || R == 16, "radix");
-    if (R == 1) return;
-    constexpr int B = ilog2(R);
-    cplx<real> y[R];
+    static_assert(R == 1 || R == 2 || R == 4 || R == 8 || R == 16 || R == 3 || R == 6 || R == 12 || R == 24 ||
+                  R == 48, "radix");
+    if constexpr (R == 1) {
+        return;
+    } else if constexpr (R % 3 == 0) {
+        constexpr int Q = R / 3;
+        cplx<real> a[3][Q];
 #pragma unroll
-    for (int q = 0; q < R; ++q) y[bitrev(q, B)] = x[q];
+        for (int n2 = 0; n2 < Q; ++n2) {
+            cplx<real> t0 = x[n2], t1 = x[Q + n2], t2 = x[2 * Q + n2];
+            dft3<real, INV>(t0, t1, t2);
+            a[0][n2] = t0;
+            a[1][n2] = rot<real, R, INV>(t1, n2);
+            a[2][n2] = rot<real, R, INV>(t2, 2 * n2);
+        }
 #pragma unroll
-    for (int m = 2; m <= R; m *= 2) {
+        for (int k1 = 0; k1 < 3; ++k1) {
+            small_dft<real, Q, INV>(a[k1]);
 #pragma unroll
-        for (int g = 0; g < R; g += m) {
+            for (int k2 = 0; k2 < Q; ++k2) x[k1 + 3 * k2] = a[k1][k2];
+        }
+    } else {
+        constexpr int B = ilog2(R);
+        cplx<real> y[R];
 #pragma unroll
-            for (int k = 0; k < m / 2; ++k) {
-                cplx<real> a = y[g + k], b = y[g + k + m / 2];
-                const int tk = k * (16 / m);   // W_m^k = W_16^{k*16/m}
-                if (tk == 0) {
-                } else if (tk == 4) {
-                    b = INV ? cmul_i(b) : cmul_mi(b);
-                } else {
-                    cplx<real> w = mk<real>((real)cos16(tk), (real)(INV ? sin16(tk) : -sin16(tk)));
-                    b = cmul(b, w);
+        for (int q = 0; q < R; ++q) y[bitrev(q, B)] = x[q];
+#pragma unroll
+        for (int m = 2; m <= R; m *= 2) {
+#pragma unroll
+            for (int g = 0; g < R; g += m) {
+#pragma unroll
+                for (int k = 0; k < m / 2; ++k) {
+                    cplx<real> a = y[g + k], b = rot<real, 16, INV>(y[g + k + m / 2], k * (16 / m));   // W_m^k
+                    y[g + k] = cadd(a, b);
+                    y[g + k + m / 2] = csub(a, b);
                 }
-                y[g + k] = cadd(a, b);
-                y[g + k + m / 2] = csub(a, b);
             }
         }
-    }
 #pragma unroll
-    for (int q = 0; q < R; ++q) x[q] = y[q];
+        for (int q = 0; q < R; ++q) x[q] = y[q];
+    }
 }
 
 // Where register slot (s + r*NB) of thread t lands after the pass above.
@@ -116,14 +165,26 @@ QAF_HD int stockham_dest(int t, int slot) {
 // ---------------------------------------------------------------------------
 QAF_HD int swz(int a) { return a ^ (((a >> 4) * 5) & 15); }
 
-// Radix schedule for L = 2^m with E = 2^e values per thread: as many radix-E
-// passes as fit, then one smaller pass for the remainder.
+// Radix schedule of a length-L transform with E values per thread.
+//   L = 2^m, E = 2^e:        as many radix-E passes as fit, then one smaller
+//                            pass for the remainder.
+//   L = 3 * 2^m, E = 3 * 2^e: one radix-E pass (it carries the factor 3),
+//                            then the power-of-two passes of L / E with
+//                            radix 2^e and a remainder.
+// Every radix divides E, so each pass is E / R butterflies per thread.
 template <int L, int E>
 struct Sched {
-    static constexpr int full = ilog2(L) / ilog2(E);
-    static constexpr int rem = 1 << (ilog2(L) - full * ilog2(E));
-    static constexpr int passes = full + (rem > 1 ? 1 : 0);
-    QAF_HD static constexpr int radix(int p) { return p < full ? E : rem; }
+    static constexpr bool R3 = L % 3 == 0;
+    static_assert(R3 ? (E % 3 == 0 && is_pow2(L / 3) && is_pow2(E / 3)) : (is_pow2(L) && is_pow2(E)),
+                  "L = 2^m with E = 2^e, or L = 3*2^m with E = 3*2^e");
+    static_assert(L % E == 0, "E divides L");
+    static constexpr int P2 = R3 ? E / 3 : E;           // radix of the power-of-two passes
+    static constexpr int L2 = R3 ? L / E : L;           // length they cover
+    static constexpr int first = R3 ? 1 : 0;
+    static constexpr int full = P2 > 1 ? ilog2(L2) / ilog2(P2) : 0;
+    static constexpr int rem = L2 >> (full * ilog2(P2 > 1 ? P2 : 2));
+    static constexpr int passes = first + full + (rem > 1 ? 1 : 0);
+    QAF_HD static constexpr int radix(int p) { return (R3 && p == 0) ? E : (p < first + full ? P2 : rem); }
     QAF_HD static constexpr int span(int p) {
         int s = 1;
         for (int q = 0; q < p; ++q) s *= radix(q);

@@ -52,8 +52,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned* flags) {
-    for (int it = 0; it < (1 << 22); ++it)
+// at most `polls` tries (0: kDefaultPolls; a test lowers it); on a timeout,
+// FLAG_WAIT_TIMEOUT in *flags (when given) and false
+constexpr unsigned kDefaultPolls = 1u << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned* flags, unsigned polls = 0) {
+    const unsigned lim = polls ? polls : kDefaultPolls;
+    for (unsigned it = 0; it < lim; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     if (flags) atomicOr(flags, FLAG_WAIT_TIMEOUT);
     return false;
@@ -68,6 +72,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsign
 // Every slab an item reads (G arrays, old, acc) is fetched by one TMA bulk
 // copy into a ring of three shared-memory buffers, issued up to three slabs
 // ahead; a y-FFT runs in the buffer its input arrived in.
+//
+// A wait that runs out (a copy that never lands) marks the CTA aborted in
+// shared memory: its later waits return at once, the CTA finishes the item it
+// is on (on whatever the buffers hold), leaves the work loop at the next item
+// boundary — where every thread reads the mark after the same barrier, so no
+// barrier is left unmatched — and waits, bounded again, for the copies it has
+// in flight before it exits. The other CTAs take the remaining items; the
+// host sees FLAG_WAIT_TIMEOUT.
 // ---------------------------------------------------------------------------
 template <typename real, int N, int E>
 struct ColKernel {
@@ -100,6 +112,7 @@ struct ColKernel {
     int t, w;
     cplx<real>* bufs;      // three slab buffers back to back
     uint64_t* mbar;        // one mbarrier per buffer
+    volatile int* aborted; // shared: a wait of this CTA ran out
     unsigned parity;       // bit b: parity of buffer b's latest issue
     // the current item: fields fa (and fb), tile T; slab sequence per field:
     // its G arrays (none in the prologue), then old and/or acc
@@ -108,6 +121,9 @@ struct ColKernel {
     int inst;              // instance of the current item
     size_t io;             // its buffer offset (complex elements)
     double* red;           // per-warp diagnostic partial sums (the edge table's space, unused by tiles)
+    int q_cur;             // queue index of the current item (test hook)
+    unsigned armed;        // thread 0: bit b, parity of buffer b's latest armed phase
+    unsigned withheld;     // thread 0: the buffer of the test hook's withheld copy (3: none)
 
     __device__ cplx<real>* buf(int b) const { return bufs + (size_t)b * SLAB; }
     __device__ int nG(int f) const { return a.mode == MODE_PROLOGUE ? 0 : (f == 0 ? 3 : 2); }
@@ -133,10 +149,19 @@ struct ColKernel {
         while (next < k) {
             const int b = next % 3;
             __syncthreads();   // every thread is done with buffer b
-            if (threadIdx.x == 0) {
+            // an aborted CTA arms nothing more: thread 0 sees the mark once its
+            // own wait for buffer b's previous slab gave up or was skipped, so
+            // no barrier is re-armed in a phase that has not completed
+            if (threadIdx.x == 0 && !*aborted) {
+                armed ^= 1u << b;
                 const unsigned bytes = (unsigned)(SLAB * sizeof(cplx<real>));
                 const int g = slab_g(next);
-                if (g >= 0) {
+                if (dropped(next)) {
+                    // test hook: the buffer is armed for the slab but the copy
+                    // is not issued, so its wait runs out (nothing in flight)
+                    expect_tx(&mbar[b], bytes);
+                    withheld = (unsigned)b;
+                } else if (g >= 0) {
                     expect_tx(&mbar[b], bytes);
                     constexpr int CPE = sizeof(cplx<real>) / 8;   // 8-byte elements per complex
 #pragma unroll 1
@@ -151,10 +176,23 @@ struct ColKernel {
             ++next;
         }
     }
+    // the test hook's slab of item 0
+    __device__ bool dropped(int sidx) const { return a.drop_slab == sidx + 1 && q_cur == 0; }
     __device__ cplx<real>* wait(int sidx) {
         const int b = sidx % 3;
-        mbar_wait(&mbar[b], ((parity >> b) & 1u) ^ 1u, a.flags);
+        // the default poll limit, or the test's lower one for the copy it withheld
+        const unsigned polls = dropped(sidx) ? a.wait_polls : 0u;
+        if (!*aborted && !mbar_wait(&mbar[b], ((parity >> b) & 1u) ^ 1u, a.flags, polls)) *aborted = 1;
         return buf(b);
+    }
+    // before an aborted CTA exits, thread 0 (which issued every copy) waits
+    // for the latest armed phase of each buffer, bounded: a consumed or
+    // never-armed buffer passes at once, a copy still in flight lands, the
+    // phase whose copy never came runs out once more
+    __device__ void drain() {
+        if (threadIdx.x == 0)
+            for (int b = 0; b < 3; ++b)
+                mbar_wait(&mbar[b], ((armed >> b) & 1u) ^ 1u, nullptr, b == (int)withheld ? a.wait_polls : 0u);
     }
 
     // forward y-FFT of slab sidx; adds ky^pow * F_y(G) to nl
@@ -566,16 +604,20 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
     cplx<real>* ctab = bufs + 3 * K::SLAB;
     uint64_t* mbar = reinterpret_cast<uint64_t*>(ctab + 2 * N);
     int* item_sh = reinterpret_cast<int*>(mbar + 3);
+    volatile int* aborted = item_sh + 1;
     const int tid = threadIdx.x, w = tid % TW, t = tid / TW;
     if (tid == 0) {
         for (int b = 0; b < 3; ++b) mbar_init(&mbar[b], 1);
+        *aborted = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     typename K::FFT fft;
     fft.template init<N>(t, a.tw);
-    K k{a, fft, t, w, bufs, mbar, 0u, 0, 0, 0, 0, 0, 0, false, false};
+    K k{a, fft, t, w, bufs, mbar, aborted, 0u, 0, 0, 0, 0, 0, 0, false, false};
     k.red = reinterpret_cast<double*>(ctab);
+    k.armed = 0u;
+    k.withheld = 3u;
     // item q of the launch: kind-major over instances (all r1+r2 tiles of all
     // instances first, then the w tiles, then the edge columns)
     const int total = K::NITEMS * a.ninst;
@@ -583,8 +625,14 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
         if (tid == 0) *item_sh = atomicAdd(a.queue, 1);
         __syncthreads();
         const int q = *item_sh;
+        const bool stop = *aborted != 0;   // written before the barrier above
         __syncthreads();
+        if (stop) {
+            k.drain();
+            break;
+        }
         if (q >= total) break;
+        k.q_cur = q;
         const int local = q / a.ninst, inst = q % a.ninst;
         if (local < K::TILES) {
             if constexpr (K::INLINE_ITEM) k.item_body(1, 2, local, inst);

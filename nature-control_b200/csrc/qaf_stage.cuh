@@ -100,6 +100,9 @@ struct alignas(64) StageArgs {
     // diagnostics / status
     double* diag;          // [0] sum w^2 weights, [1] sum |w|^2/k^2 (half plane, Parseval weights)
     unsigned* flags;       // StatusFlag bits
+    unsigned wait_polls;   // tries of a bounded copy wait before it gives up (0: the default)
+    int drop_slab;         // test hook, 0: off; k > 0: the column kernel arms slab k - 1 of
+                           // queue item 0 (always a tile) without issuing its copy
     int* queue;            // work counter of the persistent column kernel (reset by the row kernel)
     real* phys_out;        // optional: 9 physical fields + S + p11 p12 p21 (13 * N * N)
     int phys_all;          // with phys_out: also S, p11, p12, p21 (else the 9 fields only)

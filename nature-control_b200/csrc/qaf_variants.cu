@@ -54,7 +54,7 @@ struct RowV {
 
 template <class V>
 constexpr StepVariant<float> make(const char* name, int kind) {
-    return StepVariant<float>{name, kind, &V::setup, &V::launch, 0};
+    return StepVariant<float>{name, kind, &V::setup, &V::launch};
 }
 
 // "m<k>": register budget for k resident CTAs per SM (occupancy for batched small grids)

@@ -18,9 +18,10 @@ template <typename real>
 struct StepVariant {
     const char* name;   // "col:e16", "row:e8r2", ...
     int kind;           // 0: column kernel, 1: row kernel
-    cudaError_t (*setup)(int* slots);                                     // attributes; resident column CTAs
+    // attributes and resident column CTAs for the current device (the caller
+    // runs it once per device)
+    cudaError_t (*setup)(int* slots);
     void (*launch)(const StageArgs<real>& a, int slots, cudaStream_t st);
-    int slots;          // filled by setup
 };
 
 // the variants for grid size n (FP32); *out points at a static table, returns its length (0: none)

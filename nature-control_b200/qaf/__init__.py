@@ -36,6 +36,7 @@ EXPORTS = [
     "qaf_xderiv", "qaf_yderiv", "qaf_laplacian", "qaf_vel", "qaf_dealias", "qaf_if_tables", "qaf_integrate",
     "qaf_nonlinear", "qaf_step", "qaf_step_host", "qaf_last_diagnostics", "qaf_check_finite", "qaf_diagnostics",
     "qaf_state_load", "qaf_state_advance", "qaf_state_store", "qaf_last_diagnostics_async", "qaf_state_save", "qaf_state_restore", "qaf_state_advance_timed", "qaf_launch_count",
+    "qaf_test_lose_copy",
     "qaf_init_random_q", "qaf_step_noalloc", "qaf_ensemble_create", "qaf_ensemble_destroy",
     "qaf_ensemble_init_random", "qaf_ensemble_load", "qaf_ensemble_store", "qaf_ensemble_advance",
     "qaf_ensemble_diagnostics", "qaf_ensemble_set_controls", "qaf_adjoint_create", "qaf_adjoint_destroy",
@@ -134,7 +135,8 @@ def lib():
         L.qaf_launch_count.restype = ctypes.c_uint64
         L.qaf_init_random_q.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp]
         L.qaf_step_noalloc.argtypes = [cp, ctypes.c_double, ctypes.c_double, cp, ctypes.POINTER(CParams), cp,
-                                       vp, vp, vp, cp, vp]
+                                       vp, vp, vp, cp, vp, vp]
+        L.qaf_test_lose_copy.argtypes = [cp, ctypes.c_uint]
         dp = ctypes.POINTER(ctypes.c_double)
         L.qaf_ensemble_create.argtypes = [cp, ctypes.POINTER(cp), ctypes.c_double, ctypes.c_double, cp,
                                           ctypes.POINTER(CParams), dp, dp, ctypes.POINTER(vp)]

@@ -3,7 +3,6 @@ energy spectrum stay within 1% of the FP64 path's (the FP64 path matches the
 reference's own build to 1e-10 over 1000 steps, test_gpu_parity.py). Past a
 few thousand steps pointwise agreement is not expected; statistics are."""
 import math
-import os
 
 import numpy as np
 import pytest
@@ -41,7 +40,6 @@ def test_fp32_statistics_within_one_percent_of_fp64(cuda):
     assert rel.max() <= 0.01, rel.max()
 
 
-@pytest.mark.skipif(os.environ.get("QAF_LONG") != "1", reason="minutes of GPU time: set QAF_LONG=1")
 def test_fp32_statistics_at_1024_within_one_percent_of_fp64(cuda):
     # the throughput configuration (1024^2, L = 16 pi, dt = 5e-4) over 60000
     # steps (30 time units); statistics over the second half

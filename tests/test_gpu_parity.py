@@ -217,6 +217,41 @@ def test_f64_1000_steps_match_reference_build_128(cuda):
         assert O.rel_l2(host(t), g[k]) < 1e-10, k
 
 
+def _harness(tmp_path, *args):
+    """Run the reference's own CUDA build (oracle/_ref/ref_harness, the
+    unmodified reference headers in friction.cu's step order) on this GPU."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "ref_harness")
+    if not os.path.exists(exe):
+        pytest.fail(f"{exe} is missing: build it with `make -C oracle ref` where the reference tree is present")
+    out = str(tmp_path / "ref")
+    r = subprocess.run([exe, *args, "--out", out], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return out
+
+
+def test_1024_100_steps_match_reference_build_live(cuda, tmp_path):
+    # the throughput configuration (1024^2, L = 16 pi, IF-RK4, dt = 5e-4,
+    # seed 1) over 100 steps, against the reference's build run live: FP64
+    # within 1e-12 relative L2, FP32 within 1e-4. Both start from the
+    # reference's own initial spectra (its FwdTrans of the seeded fields).
+    n = 1024
+    out = _harness(tmp_path, "run", "--n", str(n), "--dt", "5e-4", "--steps", "100", "--seed", "1",
+                   "--dumps", "0,100")
+    s0 = O.read_dump(out + "_s0.bin")["fields"]
+    ref = O.read_dump(out + "_s100.bin")["fields"]
+    p = qaf.Params(dt=5e-4)
+    for dtype, bar in ((qaf.F64, 1e-12), (qaf.F32, 1e-4)):
+        m = qaf.Mesh(n, lx=L16, dtype=dtype)
+        st = [dev(a, m) for a in s0]
+        m.step(p, *st, nsteps=100)
+        m.check_finite()
+        for t, r, k in zip(st, ref, ("w", "r1", "r2")):
+            err = O.rel_l2(host(t), r)
+            assert err < bar, (dtype, k, err)
+
+
 def test_f32_100_steps_against_oracle_128(cuda):
     # FP32 path: relative L2 <= 1e-4 of the FP64 oracle after 100 steps
     n = 128
