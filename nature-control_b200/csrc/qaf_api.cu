@@ -105,6 +105,12 @@ struct DeviceOnce {
 #define QAF_ROW_THREADS 256
 #endif
 constexpr int kMinN = 16, kMaxN = 1024;
+constexpr int gcd_c(int a, int b) { return b == 0 ? a : gcd_c(b, a % b); }
+// grid sizes with kernels: powers of two in [16, 1024] and 3 * 2^k in [48, 768]
+// (the reference's own drivers run 768 = 512 * 3 / 2, friction.cu:109)
+bool size_supported(int n) {
+    return (pow2(n) && n >= kMinN && n <= kMaxN) || (n % 3 == 0 && pow2(n / 3) && n >= 48 && n <= 768);
+}
 
 // ---------------------------------------------------------------------------
 // launch configuration per (precision, N)
@@ -117,29 +123,31 @@ struct Cfg {
     static constexpr int MINB = F32 ? 2 : 1;
     // column kernel (persistent): a tile of TW kx-columns per work item, EC values
     // per thread of a length-N y-FFT
-    static constexpr int EC = QAF_COL_E < N ? QAF_COL_E : N;
+    static constexpr int EC = fit_e(N, QAF_COL_E);
     static constexpr int COL_THREADS = TW * (N / EC);
     static constexpr size_t COL_SMEM = ColKernel<real, N, EC>::SMEM;
     static constexpr int COL_ITEMS = ColKernel<real, N, EC>::NITEMS;
     // row kernel: ER values per thread of a length-N x-FFT, ROWS rows per CTA
-    static constexpr int ER = QAF_ROW_E < N ? QAF_ROW_E : N;
+    static constexpr int ER = fit_e(N, QAF_ROW_E);
     static constexpr int TEAM_R = N / ER;
     static constexpr int ROWS_A = QAF_ROW_THREADS / TEAM_R > 0 ? QAF_ROW_THREADS / TEAM_R : 1;
     static constexpr int ROWS_B = N / 8 > 0 ? N / 8 : 1;
-    static constexpr int ROWS = ROWS_A < ROWS_B ? ROWS_A : ROWS_B;
+    static constexpr int ROWS = gcd_c(N, ROWS_A < ROWS_B ? ROWS_A : ROWS_B);
     static constexpr int ROW_THREADS = ROWS * TEAM_R;
     static constexpr size_t ROW_SMEM = RowKernel<real, N, ER, ROWS>::SMEM;
     static constexpr int ROW_BLOCKS = N / ROWS;
+    static_assert(N % ROWS == 0, "rows per CTA divide the grid");
     // standalone transforms: W kx-columns per CTA, half-length row FFTs
     static constexpr int W = 4 < H ? 4 : H;
     static constexpr int COLT_THREADS = W * (N / EC);
     static constexpr size_t COLT_SMEM = (size_t)W * N * sizeof(cplx<real>);
-    static constexpr int ERT = (F32 ? 8 : 4) < H ? (F32 ? 8 : 4) : H;
+    static constexpr int ERT = fit_e(H, F32 ? 8 : 4);
     static constexpr int TEAM_T = H / ERT;
-    static constexpr int ROWS_T = (TEAM_T >= 128) ? 1 : (128 / TEAM_T <= N ? 128 / TEAM_T : N);
+    static constexpr int ROWS_T = (TEAM_T >= 128) ? 1 : gcd_c(N, 128 / TEAM_T);
     static constexpr int ROWT_THREADS = ROWS_T * TEAM_T;
     static constexpr size_t ROWT_SMEM = (size_t)ROWS_T * H * sizeof(cplx<real>);
     static constexpr int ROWT_BLOCKS = N / ROWS_T;
+    static_assert(N % ROWS_T == 0, "rows per CTA divide the grid");
 };
 
 template <typename real>
@@ -186,7 +194,7 @@ qaf_status encode_g_map(CUtensorMap* tm, const cplx<real>* G, int N, size_t rows
     const cuuint64_t cpe = sizeof(cplx<real>) / 8;
     cuuint64_t dims[2] = {(cuuint64_t)H * cpe, (cuuint64_t)(rows ? rows : (size_t)NG * N)};
     cuuint64_t strides[1] = {(cuuint64_t)H * cpe * 8};
-    cuuint32_t box[2] = {(cuuint32_t)(TW * cpe), (cuuint32_t)(N < 256 ? N : 256)};
+    cuuint32_t box[2] = {(cuuint32_t)(TW * cpe), (cuuint32_t)g_box_rows(N)};   // the column kernel's BOXR
     cuuint32_t estr[2] = {1, 1};
     CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<cplx<real>*>(G), dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
@@ -482,11 +490,13 @@ qaf_status dispatch(const qaf_mesh* m, A&&... args) {
         QAF_CASE(QAF_ONLY_N)
 #else
         QAF_CASE(16) QAF_CASE(32) QAF_CASE(64) QAF_CASE(128) QAF_CASE(256) QAF_CASE(512) QAF_CASE(1024)
+        QAF_CASE(48) QAF_CASE(96) QAF_CASE(192) QAF_CASE(384) QAF_CASE(768)
 #endif
         default: break;
     }
 #undef QAF_CASE
-    return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size (need nx == ny, a power of two in [16, 1024])");
+    return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size (need nx == ny, a power of two in [16, 1024] "
+                                     "or 3 * 2^k in [48, 768])");
 }
 
 qaf_status check_mesh(const qaf_mesh* m) {
@@ -688,7 +698,7 @@ const char* qaf_version(void) { return "qaf-b200 0.1 (sm_100a)"; }
 const char* qaf_last_error(void) { return g_last_error.c_str(); }
 
 int qaf_supported(int n, qaf_dtype dtype) {
-    return (dtype == QAF_F32 || dtype == QAF_F64) && pow2(n) && n >= kMinN && n <= kMaxN;
+    return (dtype == QAF_F32 || dtype == QAF_F64) && size_supported(n);
 }
 
 qaf_status qaf_mesh_create(const qaf_mesh_desc* desc, qaf_mesh** out) {
@@ -1349,7 +1359,9 @@ size_t carve_instance(Workspace<real>& w, cplx<real>* b, int N) {
     w.D = b + take((size_t)PF_COUNT * N);
     w.G = b + take(NG * plane);
     w.Ed = b + take((size_t)NE * N);
-    const size_t unit = (size_t)H > 32 ? (size_t)H : 32;
+    // a multiple of H (instance k's G rows start at tensor-map row k * istride / H)
+    // and of the 32-element alignment of every buffer
+    const size_t unit = (size_t)H / gcd_c(H, 32) * 32;
     return (off + unit - 1) / unit * unit;
 }
 
@@ -1385,6 +1397,10 @@ template <> std::vector<EnsGroup<double>>& groups<double>(qaf_ensemble* e) { ret
 // call f(std::integral_constant<int, N>) for a supported N
 template <class F>
 qaf_status with_n(int N, F&& f) {
+#ifdef QAF_ONLY_N
+    if (N == QAF_ONLY_N) return f(std::integral_constant<int, QAF_ONLY_N>{});
+    return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size (a build for one size only)");
+#endif
     switch (N) {
         case 16: return f(std::integral_constant<int, 16>{});
         case 32: return f(std::integral_constant<int, 32>{});
@@ -1393,6 +1409,11 @@ qaf_status with_n(int N, F&& f) {
         case 256: return f(std::integral_constant<int, 256>{});
         case 512: return f(std::integral_constant<int, 512>{});
         case 1024: return f(std::integral_constant<int, 1024>{});
+        case 48: return f(std::integral_constant<int, 48>{});
+        case 96: return f(std::integral_constant<int, 96>{});
+        case 192: return f(std::integral_constant<int, 192>{});
+        case 384: return f(std::integral_constant<int, 384>{});
+        case 768: return f(std::integral_constant<int, 768>{});
         default: return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size");
     }
 }
@@ -1870,12 +1891,13 @@ struct OpAdjBackward {
         // T arrays); otherwise one column per CTA with 16-value teams (FP64 keeps its registers)
         constexpr bool W2 = FP && sizeof(real) == 4 && N >= 128;
         constexpr int W = FP ? (W2 ? 2 : 1) : C::W;
-        constexpr int EC = FP ? (W2 ? N / 32 : (N / 16 > 4 ? N / 16 : 4)) : C::EC;
+        constexpr int P = pow2_size(N);
+        constexpr int EC = FP ? fit_e(N, W2 ? P / 32 : (P / 16 > 4 ? P / 16 : 4)) : C::EC;
         constexpr int COL_THREADS = FP ? NGA * W * (N / EC) : W * (N / EC);
         constexpr size_t COL_SMEM = FP ? (size_t)NGA * N * (W > 1 ? W : 2) * sizeof(cplx<real>)
                                        : (size_t)W * N * sizeof(cplx<real>);
         // row pass: field-parallel, teams of H/ER threads (16 from 128^2 up)
-        constexpr int ER = H / 16 < 2 ? 2 : (H / 16 > 16 ? 16 : H / 16);
+        constexpr int ER = fit_e(H, P / 32 < 2 ? 2 : (P / 32 > 16 ? 16 : P / 32));
         constexpr int ROW_THREADS = NGA * (H / ER);
         constexpr size_t ROW_SMEM = (size_t)NGA * H * sizeof(cplx<real>);
         static DeviceOnce attrs;   // kernel attributes, per device
@@ -2449,10 +2471,11 @@ qaf_status batch_backward(qaf_adjoint_batch* B, const void* const* gT, const dou
     constexpr int H = N / 2;
     // several columns per CTA: coalesced 16-32 byte segments of the T arrays (a batch has CTAs to spare)
     constexpr int W0 = sizeof(real) == 4 ? 4 : 2;
-    constexpr int W = W0 < H ? W0 : H, EC = N / 16 > 4 ? N / 16 : 4;
+    constexpr int P = pow2_size(N);
+    constexpr int W = W0 < H ? W0 : H, EC = fit_e(N, P / 16 > 4 ? P / 16 : 4);
     constexpr int COL_THREADS = NGA * W * (N / EC);
     constexpr size_t COL_SMEM = (size_t)NGA * N * (W > 1 ? W : 2) * sizeof(cplx<real>);
-    constexpr int ER = H / 16 < 2 ? 2 : (H / 16 > 16 ? 16 : H / 16);
+    constexpr int ER = fit_e(H, P / 32 < 2 ? 2 : (P / 32 > 16 ? 16 : P / 32));
     constexpr int ROW_THREADS = NGA * (H / ER);
     constexpr size_t ROW_SMEM = (size_t)NGA * H * sizeof(cplx<real>);
     static DeviceOnce attrs;   // kernel attributes, per device
@@ -2547,12 +2570,21 @@ qaf_status batch_backward(qaf_adjoint_batch* B, const void* const* gT, const dou
 
 template <class F>
 qaf_status with_small_n(int N, F&& f) {
+#ifdef QAF_ONLY_N
+    if constexpr (QAF_ONLY_N <= 256) {
+        if (N == QAF_ONLY_N) return f(std::integral_constant<int, QAF_ONLY_N>{});
+    }
+    return fail(QAF_ERR_UNSUPPORTED, "batched adjoint: no kernels for this grid size");
+#endif
     switch (N) {
         case 16: return f(std::integral_constant<int, 16>{});
         case 32: return f(std::integral_constant<int, 32>{});
         case 64: return f(std::integral_constant<int, 64>{});
         case 128: return f(std::integral_constant<int, 128>{});
         case 256: return f(std::integral_constant<int, 256>{});
+        case 48: return f(std::integral_constant<int, 48>{});
+        case 96: return f(std::integral_constant<int, 96>{});
+        case 192: return f(std::integral_constant<int, 192>{});
         default: return fail(QAF_ERR_UNSUPPORTED, "batched adjoint: grids up to 256 x 256");
     }
 }

@@ -143,6 +143,15 @@ QAF_HD void small_dft(cplx<real>* x) {
     }
 }
 
+// Values per thread of a length-L team FFT near the power of two e: e itself
+// for L = 2^m, 3e/2 for L = 3 * 2^m (the first pass carries the factor 3);
+// never more than L. The result divides L.
+QAF_HDC int fit_e(int L, int e) {
+    return L % 3 == 0 ? (3 * e / 2 < 3 ? 3 : (3 * e / 2 <= L ? 3 * e / 2 : L)) : (e <= L ? e : L);
+}
+// The power-of-two size whose launch shapes a size L follows: L, or 2L/3 for L = 3 * 2^m.
+QAF_HDC int pow2_size(int L) { return L % 3 == 0 ? 2 * L / 3 : L; }
+
 // Where register slot (s + r*NB) of thread t lands after the pass above.
 template <int L, int E, int R, int S>
 QAF_HD int stockham_dest(int t, int slot) {

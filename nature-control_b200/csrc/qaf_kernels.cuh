@@ -103,9 +103,11 @@ struct ColKernel {
         if constexpr (PF > 1) return __ldg(p);
         else return *p;
     }
-    static constexpr int BOXR = N < 256 ? N : 256;    // rows per TMA box (at most 256)
+    static constexpr int BOXR = g_box_rows(N);         // rows per TMA box (at most 256, divides N)
+    static_assert(N % BOXR == 0 && BOXR <= 256, "TMA boxes tile a slab");
     static constexpr size_t SMEM = 3 * SLAB * sizeof(cplx<real>) + 2 * N * sizeof(cplx<real>) + 4 * sizeof(uint64_t) + 16;
     using FFT = TeamFFT<real, N, E>;
+    using X = XchgCols<real>;   // exchange layout of the tile's y-FFTs
 
     const StageArgs<real>& a;
     const FFT& fft;
@@ -198,7 +200,7 @@ struct ColKernel {
     // forward y-FFT of slab sidx; adds ky^pow * F_y(G) to nl
     __device__ void forward(int sidx, int pow, cplx<real> (&nl)[E]) {
         cplx<real>* b = wait(sidx);
-        XchgCols<real> x{b, w, TW};
+        X x{b, w, TW};
         cplx<real> v[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) v[e] = b[(t + TEAM * e) * TW + w];
@@ -330,7 +332,7 @@ struct ColKernel {
         const int sx = need_acc ? sa : so;
         if (need_old && need_acc) issue_upto(so + 4);
         if (!a.do_inverse) { issue_upto(sx + 4); return; }
-        XchgCols<real> x{buf(sx % 3), w, TW};
+        X x{buf(sx % 3), w, TW};
         x.sync();   // every thread has read its old/acc values
         const int nq = f == 0 ? 4 : 2;
         for (int qq = 0; qq < nq; ++qq) {

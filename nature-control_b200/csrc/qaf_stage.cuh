@@ -118,6 +118,14 @@ struct alignas(64) StageArgs {
     size_t diag_istride;      // doubles between instances' diagnostics (0: shared)
 };
 
+// Rows per TMA box of the G arrays: at most 256 (the box limit) and a divisor
+// of N, so that the boxes of a slab tile its N rows exactly (384 -> 128).
+QAF_HDC int g_box_rows(int N) {
+    int r = N <= 256 ? N : 256;
+    while (N % r != 0) --r;
+    return r;
+}
+
 template <typename real>
 QAF_HD real ky_of(int j, int N, real dky) { return dky * (real)(j <= N / 2 ? j : j - N); }
 

@@ -22,6 +22,11 @@ noted; seeded random Q ~ U(-0.01, 0.01), w = 0, generator include/qaf_init.h):
   dealiasw64             the same with the step of dealias/couple.cu:226-229
                          (wnew truncated, r1 and r2 not), seed 11, states at
                          steps 0 1 10 200
+  grid3                  3 * 2^k grids (radix-3 transforms; the reference's
+                         drivers run 768 = 512 * 3 / 2): one nonlinear
+                         evaluation at 96^2 and 192^2 (seeds 12 / 13) and
+                         IF-RK4 dt = 1e-3 at 96^2 and 192^2 (seeds 14 / 15),
+                         states at steps 0 1 20
   kat summary            the reference's nonlinear terms for the analytic input
                          sets of UnitTest/Nonlinear/nlterms0-4 (N = 128, L = 2 pi,
                          Re = Er = 0.1, Ra = 0.2), reduced to their deviation from
@@ -46,7 +51,8 @@ import oracle as O  # noqa: E402
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 TWO_PI = "6.283185307179586"
 EIGHT_PI = "25.132741228718345"
-GROUPS = ("nl", "run32", "run64", "run128", "kat", "couple64", "dealiasw64")
+GROUPS = ("nl", "run32", "run64", "run128", "kat", "couple64", "dealiasw64", "grid3")
+GRID3_STEPS = (0, 1, 20)
 COUPLE_STEPS = (0, 1, 10, 1000)
 DEALIASW_STEPS = (0, 1, 10, 200)
 
@@ -72,6 +78,12 @@ def run_harness(out, only=GROUPS):
                         "--er", "0.1", "--rf", "0.000075", "--lambda", "0.1", "--alpha", "0.2", "--dt", "0.001",
                         "--dealias", "2", "--steps", str(DEALIASW_STEPS[-1]),
                         "--dumps", ",".join(str(s) for s in DEALIASW_STEPS), "--out", f"{out}/dealiasw64"]],
+        "grid3": [[H, "nonlinear", "--n", "96", "--init", "random", "--seed", "12", "--out", f"{out}/nl_rand96"],
+                  [H, "nonlinear", "--n", "192", "--init", "random", "--seed", "13", "--out", f"{out}/nl_rand192"],
+                  [H, "run", "--n", "96", "--steps", "20", "--seed", "14", "--dumps",
+                   ",".join(str(s) for s in GRID3_STEPS), "--out", f"{out}/run96"],
+                  [H, "run", "--n", "192", "--steps", "20", "--seed", "15", "--dumps",
+                   ",".join(str(s) for s in GRID3_STEPS), "--out", f"{out}/run192"]],
     }
     for name in only:
         for c in jobs[name]:
@@ -137,6 +149,11 @@ def convert(d, only=GROUPS):
         save("ref_couple64.npz", **states("couple64", COUPLE_STEPS))
     if "dealiasw64" in only:
         save("ref_dealiasw64.npz", **states("dealiasw64", DEALIASW_STEPS))
+    if "grid3" in only:
+        for n in (96, 192):
+            i, nl = f(f"nl_rand{n}_in.bin"), f(f"nl_rand{n}_nl.bin")
+            save(f"ref_nl_rand{n}.npz", w=i[0], r1=i[1], r2=i[2], wn=nl[0], r1n=nl[1], r2n=nl[2])
+            save(f"ref_run{n}.npz", **states(f"run{n}", GRID3_STEPS))
     if "kat" not in only:
         return
     summary = {}

@@ -3,8 +3,12 @@
 // friction.cu:212-259 launched kernel by kernel, then the same steps through
 // the library's fused path (qaf_step), compared field by field.
 //
-//   compat_driver <N> <nsteps> <integrator: rk4|rk2|ife>
+//   compat_driver <N> <nsteps> <integrator: rk4|rk2|ife> [params: test|friction]
 // prints one JSON line {"rel_w": .., "rel_r1": .., "rel_r2": .., "energy": ..}.
+// params "friction" takes friction.cu's own settings (friction.cu:100-117:
+// lambda 0.1, Rf 0.00075, alpha 0.2, Re = Er = 0.1, dt 0.002, Lx = 33 * 2 pi,
+// with its Nx = 512 * 3 / 2 = 768 given as N); "test" (the default) Lx = 16 pi,
+// Re = Er = 1, Rf = 0.1, alpha 1, dt 1e-3.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -34,9 +38,11 @@ int main(int argc, char** argv) {
     const int Nx = argc > 1 ? std::atoi(argv[1]) : 64;
     const int Ns = argc > 2 ? std::atoi(argv[2]) : 10;
     const std::string integ = argc > 3 ? argv[3] : "rk4";
+    const bool friction = argc > 4 && std::string(argv[4]) == "friction";
     const int Ny = Nx, BSZ = 16, Nxh = Nx / 2 + 1;
-    const Qreal Lx = 16 * M_PI, Ly = Lx;
-    const Qreal lambda = 0.1, Rf = 0.1, alpha = 1.0, Re = 1.0, Er = 1.0, dt = 1e-3;
+    const Qreal Lx = friction ? 33 * 2 * M_PI : 16 * M_PI, Ly = Lx;
+    const Qreal lambda = 0.1, Rf = friction ? 0.00075 : 0.1, alpha = friction ? 0.2 : 1.0;
+    const Qreal Re = friction ? 0.1 : 1.0, Er = friction ? 0.1 : 1.0, dt = friction ? 0.002 : 1e-3;
 
     Mesh* mesh = new Mesh(Nx, Ny, Lx, Ly, BSZ);
     Field *wold = new Field(mesh), *wcurr = new Field(mesh), *wnew = new Field(mesh), *wnonl = new Field(mesh);

@@ -74,7 +74,7 @@ double check() {
 int main() {
     int bad = 0;
     // the exchange swizzle permutes every buffer length the kernels use (8 .. 8192 elements)
-    for (int len = 8; len <= 8192; len *= 2) {
+    for (int len = 8; len <= 8192; len = (len % 3 == 0) ? len * 4 / 3 : (len >= 16 ? len * 3 / 2 : len * 2)) {
         std::vector<int> seen(len, 0);
         for (int a = 0; a < len; ++a) {
             const int p = swz(a);
@@ -87,6 +87,14 @@ int main() {
     CASE(double, 512, 8, false, 1e-14); CASE(double, 1024, 8, true, 1e-14);
     CASE(double, 1024, 16, false, 1e-14); CASE(double, 2048, 8, false, 1e-14);
     CASE(float, 64, 8, false, 1e-6); CASE(float, 512, 8, true, 1e-6); CASE(float, 1024, 4, false, 1e-6);
+    // lengths 3 * 2^m (the reference's 768 = 512 * 3 / 2 and its divisors), radix-3E first pass
+    CASE(double, 3, 3, false, 1e-14); CASE(double, 6, 6, true, 1e-14); CASE(double, 12, 12, false, 1e-14);
+    CASE(double, 24, 24, true, 1e-14); CASE(double, 48, 48, false, 1e-14); CASE(double, 48, 12, true, 1e-14);
+    CASE(double, 96, 12, false, 1e-14); CASE(double, 96, 24, true, 1e-14); CASE(double, 192, 12, true, 1e-14);
+    CASE(double, 384, 12, false, 1e-14); CASE(double, 384, 24, false, 1e-14); CASE(double, 768, 12, true, 1e-14);
+    CASE(double, 768, 24, false, 1e-14); CASE(double, 768, 48, true, 1e-14); CASE(double, 1536, 12, false, 1e-14);
+    CASE(double, 96, 6, false, 1e-14); CASE(double, 768, 6, true, 1e-14);
+    CASE(float, 768, 12, false, 2e-6); CASE(float, 384, 24, true, 2e-6); CASE(float, 96, 12, false, 2e-6);
     std::printf(bad ? "FAIL\n" : "PASS\n");
     return bad ? 1 : 0;
 }

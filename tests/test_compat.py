@@ -48,6 +48,18 @@ def test_reference_style_loop_matches_fused_step_fp64(cuda, integ, n, steps):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fp32,bar", [(False, 1e-12), (True, 1e-5)])
+def test_friction_driver_settings_768(cuda, fp32, bar):
+    # friction.cu's own grid and parameters: Nx = 512 * 3 / 2 = 768, Lx = 66 pi,
+    # Re = Er = 0.1, Rf = 0.00075, alpha = 0.2, dt = 0.002
+    r = subprocess.run([_build(fp32), "768", "10", "rk4", "friction"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    for k in ("rel_w", "rel_r1", "rel_r2"):
+        assert out[k] <= bar, out
+
+
+@pytest.mark.gpu
 def test_reference_style_loop_matches_fused_step_fp32(cuda):
     r = subprocess.run([_build(True), "64", "20", "rk4"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]

@@ -16,6 +16,8 @@ pytestmark = pytest.mark.gpu
 
 L16 = 16 * np.pi
 SIZES = [16, 32, 64, 128, 256, 512, 1024]
+# 3 * 2^k grids (radix-3 first pass): the reference's drivers run 768 = 512 * 3 / 2
+SIZES3 = [48, 96, 192, 384, 768]
 
 
 def dev(a, mesh):
@@ -43,7 +45,7 @@ def random_spec(n, seed, hermitian=False):
 
 
 @pytest.mark.parametrize("dtype", [qaf.F64, qaf.F32])
-@pytest.mark.parametrize("n", SIZES)
+@pytest.mark.parametrize("n", SIZES + SIZES3)
 def test_transforms_against_oracle(cuda, n, dtype):
     m = qaf.Mesh(n, lx=L16, dtype=dtype)
     rng = np.random.default_rng(n)
@@ -124,7 +126,7 @@ def test_if_tables_and_stage_kernels(cuda, dtype, integ, stages):
 
 
 @pytest.mark.parametrize("dtype", [qaf.F64, qaf.F32])
-@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512])
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512, 48, 96, 192, 384, 768])
 def test_nonlinear_against_oracle(cuda, n, dtype):
     # full-spectrum input with non-Hermitian kx = 0 and kx = n/2 columns, as in RK stages 2-4
     m = qaf.Mesh(n, lx=L16, dtype=dtype)
@@ -152,7 +154,7 @@ def test_nonlinear_physical_fields_against_oracle(cuda):
         assert O.rel_l2(gph[gi], oph[oi]) < 1e-13, (oi, gi)
 
 
-@pytest.mark.parametrize("n", [32, 64])
+@pytest.mark.parametrize("n", [32, 64, 96, 192])
 def test_nonlinear_against_reference_build(cuda, n):
     g = golden(f"ref_nl_rand{n}.npz")
     m = qaf.Mesh(n, lx=L16, dtype=qaf.F64)
@@ -174,7 +176,7 @@ def test_nonlinear_known_answers_gpu(cuda, k):
 
 
 @pytest.mark.parametrize("integ", [qaf.IFRK4, qaf.IFRK2, qaf.IFE])
-@pytest.mark.parametrize("n", [16, 32, 64, 128])
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 48, 96, 192])
 def test_steps_against_oracle_f64(cuda, n, integ):
     m = qaf.Mesh(n, lx=L16, dtype=qaf.F64)
     p = O.params(n=n)
@@ -184,6 +186,21 @@ def test_steps_against_oracle_f64(cuda, n, integ):
     m.step(qaf.Params(), *st, nsteps=5, integrator=integ)
     for g, o in zip(st, ref):
         assert O.rel_l2(host(g), o) < 1e-13
+
+
+@pytest.mark.parametrize("n", [96, 192])
+def test_rk4_matches_reference_build_3x2k(cuda, n):
+    # radix-3 grids against the reference's build (golden grid3 group)
+    g = golden(f"ref_run{n}.npz")
+    for dtype, bar in ((qaf.F64, 1e-13), (qaf.F32, 2e-5)):
+        m = qaf.Mesh(n, lx=L16, dtype=dtype)
+        st = [dev(g[f"{k}_0"], m) for k in ("w", "r1", "r2")]
+        prev = 0
+        for s in (1, 20):
+            m.step(qaf.Params(), *st, nsteps=s - prev)
+            prev = s
+            for t, k in zip(st, ("w", "r1", "r2")):
+                assert O.rel_l2(host(t), g[f"{k}_{s}"]) < bar, (dtype, s, k)
 
 
 def test_rk4_matches_reference_build_32_and_64(cuda):
@@ -252,6 +269,27 @@ def test_1024_100_steps_match_reference_build_live(cuda, tmp_path):
             assert err < bar, (dtype, k, err)
 
 
+@pytest.mark.parametrize("dtype,bar", [(qaf.F64, 1e-12), (qaf.F32, 1e-4)])
+def test_768_friction_settings_match_reference_build_live(cuda, tmp_path, dtype, bar):
+    # the reference driver's own grid and parameters (friction.cu:100-117):
+    # 768^2, L = 66 pi, Re = Er = 0.1, Rf = 0.00075, alpha = 0.2, lambda = 0.1,
+    # dt = 0.002; seeded random Q (the driver reads its initial CSVs, absent
+    # here); 100 steps against the reference's build run live
+    n, L66 = 768, 66 * np.pi
+    out = _harness(tmp_path, "run", "--n", str(n), "--L", repr(L66), "--re", "0.1", "--er", "0.1",
+                   "--rf", "0.00075", "--alpha", "0.2", "--lambda", "0.1", "--dt", "0.002", "--steps", "100",
+                   "--seed", "6", "--dumps", "0,100")
+    s0 = O.read_dump(out + "_s0.bin")["fields"]
+    ref = O.read_dump(out + "_s100.bin")["fields"]
+    m = qaf.Mesh(n, lx=L66, dtype=dtype)
+    st = [dev(a, m) for a in s0]
+    m.step(qaf.Params(re=0.1, er=0.1, rf=0.00075, alpha=0.2, lam=0.1, dt=0.002), *st, nsteps=100)
+    m.check_finite()
+    for t, r, k in zip(st, ref, ("w", "r1", "r2")):
+        err = O.rel_l2(host(t), r)
+        assert err < bar, (k, err)
+
+
 def test_f32_100_steps_against_oracle_128(cuda):
     # FP32 path: relative L2 <= 1e-4 of the FP64 oracle after 100 steps
     n = 128
@@ -294,7 +332,8 @@ def test_alpha_field_and_variants_against_oracle(cuda):
 
 def test_taylor_green_decay_gpu(cuda):
     # FP32: |w| ~ 2 and 20 steps of float rounding
-    for n, dtype, t in ((64, qaf.F64, 1e-13), (1024, qaf.F64, 1e-12), (1024, qaf.F32, 1e-5)):
+    for n, dtype, t in ((64, qaf.F64, 1e-13), (1024, qaf.F64, 1e-12), (1024, qaf.F32, 1e-5),
+                        (768, qaf.F64, 1e-12), (768, qaf.F32, 1e-5)):
         m = qaf.Mesh(n, lx=2 * np.pi, dtype=dtype)
         x = np.arange(n) * 2 * np.pi / n
         X, Y = np.meshgrid(x, x)
@@ -370,10 +409,11 @@ def test_invalid_arguments_are_rejected(cuda):
         m.step(qaf.Params(), *st, integrator=7)
     with pytest.raises(ValueError):
         m.step(qaf.Params(), st[0][:, :5].contiguous(), st[1], st[2])
-    m48 = qaf.Mesh(48, lx=L16, dtype=qaf.F64)
-    s48 = [m48.new_spec() for _ in range(3)]
+    # 80 = 5 * 16: neither a power of two nor 3 * 2^k
+    m80 = qaf.Mesh(80, lx=L16, dtype=qaf.F64)
+    s80 = [m80.new_spec() for _ in range(3)]
     with pytest.raises(qaf.QafError) as e:
-        m48.step(qaf.Params(), *s48)
+        m80.step(qaf.Params(), *s80)
     assert e.value.status == qaf.ERR_UNSUPPORTED
 
 

@@ -48,7 +48,11 @@ def test_library_host_only_calls(lib):
     import qaf
     assert "sm_100a" in qaf.version()
     assert qaf.supported(1024, qaf.F32) and qaf.supported(128, qaf.F64)
-    assert not qaf.supported(48, qaf.F32) and not qaf.supported(2048, qaf.F32)
+    # powers of two in [16, 1024] and 3 * 2^k in [48, 768] (the reference's 768 = 512 * 3 / 2)
+    for n in (48, 96, 192, 384, 768):
+        assert qaf.supported(n, qaf.F32) and qaf.supported(n, qaf.F64), n
+    for n in (2048, 1536, 24, 12, 80, 100):
+        assert not qaf.supported(n, qaf.F32), n
     h = ctypes.c_void_p()
     bad = qaf.MeshDesc(7, 8, 1.0, 1.0, qaf.F64)
     assert lib.qaf_mesh_create(ctypes.byref(bad), ctypes.byref(h)) == qaf.ERR_INVALID

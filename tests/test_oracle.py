@@ -107,7 +107,7 @@ def test_nonlinear_known_answers(k):
         assert a < 10 * b + 1e-13
 
 
-@pytest.mark.parametrize("n", [32, 64])
+@pytest.mark.parametrize("n", [32, 64, 96, 192])
 def test_nonlinear_matches_reference_build(n):
     g = golden(f"ref_nl_rand{n}.npz")
     p = O.params(n=n)
@@ -130,6 +130,24 @@ def test_rk4_steps_match_reference_build_32():
     st = (g["w_0"], g["r1_0"], g["r2_0"])
     prev = 0
     for s in (1, 2, 10, 20):
+        st = O.step(p, *st, s - prev)
+        prev = s
+        for a, name in zip(st, ("w", "r1", "r2")):
+            assert O.rel_l2(a, g[f"{name}_{s}"]) < 1e-14, (s, name)
+
+
+@pytest.mark.parametrize("n", [96, 192])
+def test_rk4_steps_match_reference_build_3x2k(n):
+    # 3 * 2^k grids: the oracle's mixed-radix transform against the reference's
+    # build (cuFFT), including its initial FwdTrans of the seeded fields
+    g = golden(f"ref_run{n}.npz")
+    p = O.params(n=n)
+    w, r1, r2 = O.initial_spectra(14 if n == 96 else 15, n)
+    for a, name in zip((w, r1, r2), ("w_0", "r1_0", "r2_0")):
+        assert O.rel_l2(O.hermitian_part(a), O.hermitian_part(g[name])) < 1e-15
+    st = (g["w_0"], g["r1_0"], g["r2_0"])
+    prev = 0
+    for s in (1, 20):
         st = O.step(p, *st, s - prev)
         prev = s
         for a, name in zip(st, ("w", "r1", "r2")):
