@@ -48,7 +48,7 @@ typedef enum { QAF_F32 = 0, QAF_F64 = 1 } qaf_dtype;
 typedef enum { QAF_IFE = 0, QAF_IFRK2 = 1, QAF_IFRK4 = 2 } qaf_integrator;
 
 typedef struct {
-    int nx, ny;        /* grid points (nx even); the fused stepper needs nx == ny */
+    int nx, ny;        /* grid points; each a size qaf_supported accepts (nx != ny allowed) */
     double lx, ly;     /* domain lengths */
     qaf_dtype dtype;
 } qaf_mesh_desc;
@@ -75,7 +75,8 @@ typedef struct qaf_mesh qaf_mesh;
 const char* qaf_version(void);
 /* message of the last failing call on this host thread ("" if none) */
 const char* qaf_last_error(void);
-/* 1 if the fused stepper has kernels for an n x n grid of this dtype */
+/* 1 if there are kernels for grid size n (as nx or as ny) in this dtype: powers
+ * of two in [16, 1024] and 3 * 2^k in [48, 768] */
 int qaf_supported(int n, qaf_dtype dtype);
 
 /* ---- mesh (Basic/Mesh.cuh:48-113; Field :115-129) ---------------------- */

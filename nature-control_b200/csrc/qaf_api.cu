@@ -104,8 +104,13 @@ struct DeviceOnce {
 #ifndef QAF_ROW_THREADS
 #define QAF_ROW_THREADS 256
 #endif
+#ifndef QAF_COL1024_MODE
+#define QAF_COL1024_MODE 18
+#endif
 constexpr int kMinN = 16, kMaxN = 1024;
 constexpr int gcd_c(int a, int b) { return b == 0 ? a : gcd_c(b, a % b); }
+// the largest power of two <= min(x, cap)
+constexpr int pow2_floor(int x, int cap) { return (x > cap ? cap : x) <= 1 ? 1 : 2 * pow2_floor((x > cap ? cap : x) / 2, cap); }
 // grid sizes with kernels: powers of two in [16, 1024] and 3 * 2^k in [48, 768]
 // (the reference's own drivers run 768 = 512 * 3 / 2, friction.cu:109)
 bool size_supported(int n) {
@@ -121,33 +126,46 @@ struct Cfg {
     static constexpr bool F32 = sizeof(real) == 4;
     // CTAs per SM the register budget is sized for (FP64 kernels need > 128 registers)
     static constexpr int MINB = F32 ? 2 : 1;
-    // column kernel (persistent): a tile of TW kx-columns per work item, EC values
-    // per thread of a length-N y-FFT
+    // values per thread of a length-N y-FFT (standalone transforms, adjoint)
     static constexpr int EC = fit_e(N, QAF_COL_E);
-    static constexpr int COL_THREADS = TW * (N / EC);
-    static constexpr size_t COL_SMEM = ColKernel<real, N, EC>::SMEM;
-    static constexpr int COL_ITEMS = ColKernel<real, N, EC>::NITEMS;
+    // the step's column kernel (persistent): a tile of TW kx-columns per work
+    // item, ECS values per thread, MINBC CTAs per SM for the register budget,
+    // and the ColKernel mode: at 1024^2 FP32 the shared twiddle table, the
+    // double-buffered swizzled exchange and the ky table in shared memory
+    // with 4 values per thread in one 1024-thread CTA per SM (no spills at
+    // 64 registers); the shared twiddle table (mode 1) for FP32 768^2, FP64
+    // from 512^2 and every batch (ensemble) launch; otherwise register
+    // twiddle bases (mode 0: for single small grids, whose launches are
+    // latency-bound, the table's fill at kernel start measured slower)
+    static constexpr bool WIDE1024 = F32 && N == 1024;
+    static constexpr int ECS = WIDE1024 ? 4 : EC;
+    static constexpr int COL_MODE = WIDE1024 ? QAF_COL1024_MODE : (((F32 && N == 768) || (!F32 && N >= 512)) ? 1 : 0);
+    static constexpr int COL_MODE_B = WIDE1024 ? QAF_COL1024_MODE : 1;   // batches of instances
+    static constexpr int MINBC = WIDE1024 ? 1 : MINB;
+    static constexpr int COL_THREADS = TW * (N / ECS);
+    static constexpr size_t COL_SMEM = ColKernel<real, N, ECS, COL_MODE>::SMEM;
+    static constexpr size_t COL_SMEM_B = ColKernel<real, N, ECS, COL_MODE_B>::SMEM;
     // row kernel: ER values per thread of a length-N x-FFT, ROWS rows per CTA
     static constexpr int ER = fit_e(N, QAF_ROW_E);
     static constexpr int TEAM_R = N / ER;
     static constexpr int ROWS_A = QAF_ROW_THREADS / TEAM_R > 0 ? QAF_ROW_THREADS / TEAM_R : 1;
     static constexpr int ROWS_B = N / 8 > 0 ? N / 8 : 1;
-    static constexpr int ROWS = gcd_c(N, ROWS_A < ROWS_B ? ROWS_A : ROWS_B);
+    // a power of two of at most 16, so that it divides the row count ny of any
+    // supported grid (all multiples of 16), not only N
+    static constexpr int ROWS = pow2_floor(gcd_c(N, ROWS_A < ROWS_B ? ROWS_A : ROWS_B), 16);
     static constexpr int ROW_THREADS = ROWS * TEAM_R;
     static constexpr size_t ROW_SMEM = RowKernel<real, N, ER, ROWS>::SMEM;
-    static constexpr int ROW_BLOCKS = N / ROWS;
-    static_assert(N % ROWS == 0, "rows per CTA divide the grid");
+    static_assert(16 % ROWS == 0, "rows per CTA divide every row count");
     // standalone transforms: W kx-columns per CTA, half-length row FFTs
     static constexpr int W = 4 < H ? 4 : H;
     static constexpr int COLT_THREADS = W * (N / EC);
     static constexpr size_t COLT_SMEM = (size_t)W * N * sizeof(cplx<real>);
     static constexpr int ERT = fit_e(H, F32 ? 8 : 4);
     static constexpr int TEAM_T = H / ERT;
-    static constexpr int ROWS_T = (TEAM_T >= 128) ? 1 : gcd_c(N, 128 / TEAM_T);
+    static constexpr int ROWS_T = (TEAM_T >= 128) ? 1 : pow2_floor(gcd_c(N, 128 / TEAM_T), 16);
     static constexpr int ROWT_THREADS = ROWS_T * TEAM_T;
     static constexpr size_t ROWT_SMEM = (size_t)ROWS_T * H * sizeof(cplx<real>);
-    static constexpr int ROWT_BLOCKS = N / ROWS_T;
-    static_assert(N % ROWS_T == 0, "rows per CTA divide the grid");
+    static_assert(16 % ROWS_T == 0, "rows per CTA divide every row count");
 };
 
 template <typename real>
@@ -163,7 +181,8 @@ struct Workspace {
     cplx<real>* G;
     cplx<real>* Ed;
     cplx<real>* T;     // transform scratch
-    cplx<real>* tw;
+    cplx<real>* tw;    // twiddles of length nx (row transforms)
+    cplx<real>* tw_y;  // twiddles of length ny (column transforms; == tw when nx == ny)
     real* ex;
     real* ey;
     double* diag;      // [0] energy sum, [1] enstrophy sum, [2..] spectrum shells (scratch)
@@ -176,10 +195,11 @@ struct Workspace {
 
 size_t align_up(size_t x) { return (x + 31) & ~size_t(31); }
 
-// TMA descriptor of the G arrays: [NG*N rows][H columns] of 8-byte elements
-// (two per FP64 complex), boxes of TW columns x min(N, 256) rows.
+// TMA descriptor of the G arrays: [NG*ny rows][nx/2 columns] of 8-byte
+// elements (two per FP64 complex), boxes of TW columns x g_box_rows(ny) rows
+// (rows: the total row count when several instances follow each other).
 template <typename real>
-qaf_status encode_g_map(CUtensorMap* tm, const cplx<real>* G, int N, size_t rows = 0) {
+qaf_status encode_g_map(CUtensorMap* tm, const cplx<real>* G, int nx, int ny, size_t rows = 0) {
     // looked up once per process (a function-local static: thread-safe)
     static const PFN_cuTensorMapEncodeTiled_v12000 encode = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
         cudaDriverEntryPointQueryResult q;
@@ -190,11 +210,11 @@ qaf_status encode_g_map(CUtensorMap* tm, const cplx<real>* G, int N, size_t rows
         return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }();
     if (!encode) return fail(QAF_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    const int H = N / 2;
+    const int H = nx / 2;
     const cuuint64_t cpe = sizeof(cplx<real>) / 8;
-    cuuint64_t dims[2] = {(cuuint64_t)H * cpe, (cuuint64_t)(rows ? rows : (size_t)NG * N)};
+    cuuint64_t dims[2] = {(cuuint64_t)H * cpe, (cuuint64_t)(rows ? rows : (size_t)NG * ny)};
     cuuint64_t strides[1] = {(cuuint64_t)H * cpe * 8};
-    cuuint32_t box[2] = {(cuuint32_t)(TW * cpe), (cuuint32_t)g_box_rows(N)};   // the column kernel's BOXR
+    cuuint32_t box[2] = {(cuuint32_t)(TW * cpe), (cuuint32_t)g_box_rows(ny)};   // the column kernel's BOXR
     cuuint32_t estr[2] = {1, 1};
     CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<cplx<real>*>(G), dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
@@ -240,8 +260,9 @@ std::vector<cplx<real>> host_twiddles(int N) {
 // and L_Q = -kx^2 - ky^2 + q_lin factor into exp(-c kx^2 dt) exp(-c ky^2 dt) exp(c0 dt).
 // ex/ey hold the kx/ky factors for the classes {w full, w half, Q full, Q half} step.
 template <typename real>
-void host_if_tables(int N, double dkx, double dky, double dt, double re, std::vector<real>& ex, std::vector<real>& ey) {
-    const int H = N / 2;
+void host_if_tables(int nx, int ny, double dkx, double dky, double dt, double re, std::vector<real>& ex,
+                    std::vector<real>& ey) {
+    const int H = nx / 2, N = ny;
     ex.assign(4 * (H + 1), 0);
     ey.assign(4 * (size_t)N, 0);
     const double steps[4] = {dt, 0.5 * dt, dt, 0.5 * dt};
@@ -271,7 +292,8 @@ template <typename real>
 qaf_status ensure_ws(qaf_mesh* m) {
     Workspace<real>& w = ws<real>(m);
     if (w.block) return QAF_OK;
-    const int N = m->desc.nx, H = N / 2;
+    // columns of length N = ny, H = nx / 2 of them (the state's main part)
+    const int NXg = m->desc.nx, N = m->desc.ny, H = NXg / 2;
     const size_t plane = (size_t)N * H;
     // element counts (complex)
     size_t off = 0;
@@ -280,7 +302,7 @@ qaf_status ensure_ws(qaf_mesh* m) {
     for (int f = 0; f < 3; ++f) { o_old_m[f] = take(plane); o_old_n[f] = take(N); }
     for (int f = 0; f < 3; ++f) { o_acc_m[f] = take(plane); o_acc_n[f] = take(N); }
     size_t oY = take(NY * plane), oD = take((size_t)PF_COUNT * N), oG = take(NG * plane), oE = take((size_t)NE * N);
-    size_t oT = take(plane), otw = take(N);
+    size_t oT = take(plane), otw = take(NXg), otwy = take(N);
     // real tables stored in complex slots
     size_t oex = take((4 * (H + 1) + 1) / 2 + 1), oey = take((4 * N + 1) / 2 + 1);
     // [0, 2) step sums, [2, 4) diagnostics, [4, 516) spectrum, [516, 1029) shell bounds, [1029, 1031) async copy-out
@@ -296,15 +318,16 @@ qaf_status ensure_ws(qaf_mesh* m) {
         w.old_m[f] = b + o_old_m[f]; w.old_n[f] = b + o_old_n[f];
         w.acc_m[f] = b + o_acc_m[f]; w.acc_n[f] = b + o_acc_n[f];
     }
-    w.Y = b + oY; w.D = b + oD; w.G = b + oG; w.Ed = b + oE; w.T = b + oT; w.tw = b + otw;
+    w.Y = b + oY; w.D = b + oD; w.G = b + oG; w.Ed = b + oE; w.T = b + oT; w.tw = b + otw; w.tw_y = b + otwy;
     w.ex = reinterpret_cast<real*>(b + oex);
     w.ey = reinterpret_cast<real*>(b + oey);
     w.diag = reinterpret_cast<double*>(b + odiag);
     w.flags = reinterpret_cast<unsigned*>(b + oflags);
     w.queue = reinterpret_cast<int*>(b + oqueue);
-    const std::vector<cplx<real>> tw = host_twiddles<real>(N);
-    QAF_CUDA(cudaMemcpy(w.tw, tw.data(), N * sizeof(cplx<real>), cudaMemcpyHostToDevice));
-    QAF_TRY(encode_g_map<real>(&w.tm_G, w.G, N));
+    const std::vector<cplx<real>> tw = host_twiddles<real>(NXg), twy = host_twiddles<real>(N);
+    QAF_CUDA(cudaMemcpy(w.tw, tw.data(), NXg * sizeof(cplx<real>), cudaMemcpyHostToDevice));
+    QAF_CUDA(cudaMemcpy(w.tw_y, twy.data(), N * sizeof(cplx<real>), cudaMemcpyHostToDevice));
+    QAF_TRY(encode_g_map<real>(&w.tm_G, w.G, NXg, N));
     QAF_CUDA(cudaMemset(w.flags, 0, sizeof(unsigned)));
     QAF_CUDA(cudaMemset(w.diag, 0, 2 * sizeof(double)));
     return QAF_OK;
@@ -315,7 +338,7 @@ qaf_status ensure_if(qaf_mesh* m, const qaf_params* p, cudaStream_t st) {
     Workspace<real>& w = ws<real>(m);
     if (w.cached[0] == p->dt && w.cached[1] == p->re && w.cached[2] == p->rf && w.cached[3] == p->q_lin) return QAF_OK;
     std::vector<real> ex, ey;
-    host_if_tables<real>(m->desc.nx, m->dkx, m->dky, p->dt, p->re, ex, ey);
+    host_if_tables<real>(m->desc.nx, m->desc.ny, m->dkx, m->dky, p->dt, p->re, ex, ey);
     host_if_e0<real>(p->dt, p->re, p->rf, p->q_lin, w.e0);
     QAF_CUDA(cudaMemcpyAsync(w.ex, ex.data(), ex.size() * sizeof(real), cudaMemcpyHostToDevice, st));
     QAF_CUDA(cudaMemcpyAsync(w.ey, ey.data(), ey.size() * sizeof(real), cudaMemcpyHostToDevice, st));
@@ -329,27 +352,27 @@ qaf_status ensure_if(qaf_mesh* m, const qaf_params* p, cudaStream_t st) {
 // (no_dealias 0, friction.cu:253-255), none (1, the coupled runs,
 // couple.cu:179-215) or w only (2, dealias/couple.cu:226-229)
 template <class Args>
-void set_mask(Args& a, int N, int no_dealias) {
-    a.kx_keep = (N / 2) * 2 / 3; a.ky_lo = N / 3; a.ky_hi = N - N / 3 + 1;
+void set_mask(Args& a, int nx, int ny, int no_dealias) {
+    a.kx_keep = (nx / 2) * 2 / 3; a.ky_lo = ny / 3; a.ky_hi = ny - ny / 3 + 1;
     a.trunc = no_dealias == 0 ? 7 : (no_dealias == 2 ? 1 : 0);
 }
 
 template <typename real>
 StageArgs<real> make_args(qaf_mesh* m, const qaf_params* p) {
     Workspace<real>& w = ws<real>(m);
-    const int N = m->desc.nx;
     StageArgs<real> a;
     std::memset(&a, 0, sizeof(a));
+    a.nx = m->desc.nx; a.ny = m->desc.ny;
     a.dkx = (real)m->dkx; a.dky = (real)m->dky;
     a.lambda = (real)p->lambda; a.ce = (real)(1.0 / (p->er * p->re)); a.alpha = (real)p->alpha;
     a.alpha_field = reinterpret_cast<const real*>(p->alpha_field);
     a.dt = (real)p->dt; a.advect = p->advect_omega ? 1 : 0;
-    set_mask(a, N, p->no_dealias);
+    set_mask(a, a.nx, a.ny, p->no_dealias);
     for (int f = 0; f < 3; ++f) {
         a.old_m[f] = w.old_m[f]; a.old_n[f] = w.old_n[f]; a.acc_m[f] = w.acc_m[f]; a.acc_n[f] = w.acc_n[f];
         a.nl_m[f] = w.acc_m[f]; a.nl_n[f] = w.acc_n[f];
     }
-    a.Y = w.Y; a.D = w.D; a.G = w.G; a.Ed = w.Ed; a.tw = w.tw; a.ex = w.ex; a.ey = w.ey;
+    a.Y = w.Y; a.D = w.D; a.G = w.G; a.Ed = w.Ed; a.tw = w.tw; a.tw_y = w.tw_y; a.ex = w.ex; a.ey = w.ey;
     for (int c = 0; c < 4; ++c) a.e0[c] = w.e0[c];
     a.diag = w.diag; a.flags = w.flags; a.queue = w.queue;
     a.tm_G = w.tm_G;
@@ -411,27 +434,44 @@ std::atomic<unsigned> g_test_polls{0};
 // ---------------------------------------------------------------------------
 // per-size launchers
 // ---------------------------------------------------------------------------
+// Launches of the kernels whose transform length is N: the row kernel and
+// row transforms of a grid with nx = N, the column kernel and column
+// transforms of a grid with ny = N (the other size is an argument).
 template <typename real, int N>
 struct Launch {
     using C = Cfg<real, N>;
-    // resident column CTAs per device (the persistent grid size)
-    static inline DeviceOnce col_slots;
+    // resident column CTAs per device (the persistent grid size) of the
+    // single-grid and the batch column kernels
+    static inline DeviceOnce col_slots, col_slots_b;
     static qaf_status setup() {
+        QAF_TRY(col_slots_b.get(nullptr, [](int* slots) -> qaf_status {
+            QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE_B>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM_B));
+            int dev = 0, sms = 0, per_sm = 0;
+            QAF_CUDA(cudaGetDevice(&dev));
+            QAF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            QAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE_B>,
+                                                                   C::COL_THREADS, C::COL_SMEM_B));
+            if (per_sm < 1) return fail(QAF_ERR_UNSUPPORTED, "column kernel does not fit on an SM");
+            *slots = sms * per_sm;
+            return QAF_OK;
+        }));
         return col_slots.get(nullptr, [](int* slots) -> qaf_status {
-            QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::EC, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
+            QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
             QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::ROW_SMEM));
             QAF_CUDA(cudaFuncSetAttribute(col_ifft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
             QAF_CUDA(cudaFuncSetAttribute(col_fft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
             int dev = 0, sms = 0, per_sm = 0;
             QAF_CUDA(cudaGetDevice(&dev));
             QAF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            QAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_kernel<real, N, C::EC, C::MINB>,
+            QAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE>,
                                                                    C::COL_THREADS, C::COL_SMEM));
             if (per_sm < 1) return fail(QAF_ERR_UNSUPPORTED, "column kernel does not fit on an SM");
             *slots = sms * per_sm;
             return QAF_OK;
         });
     }
+    // the column kernel of a grid with ny = N (a.nx / 2 / TW tiles)
     static void col(const StageArgs<real>& a0, cudaStream_t st) {
         StageArgs<real> hooked;
         const StageArgs<real>* ap = &a0;
@@ -446,40 +486,124 @@ struct Launch {
         const StageArgs<real>& a = *ap;
         if constexpr (std::is_same<real, float>::value) {
             int slots = 0;
-            if (StepVariant<float>* v = tuned_variant(N, 0, a.ninst > 1, &slots)) {
-                v->launch(a, slots, st);
-                return;
+            if (a.nx == a.ny) {
+                if (StepVariant<float>* v = tuned_variant(N, 0, a.ninst > 1, &slots)) {
+                    v->launch(a, slots, st);
+                    return;
+                }
             }
         }
-        const long items = (long)C::COL_ITEMS * a.ninst;
+        const long items = (long)(2 * (a.nx / 2 / TW) + 3) * a.ninst;
+        if (a.ninst > 1 && C::COL_MODE_B != C::COL_MODE) {
+            const int slots = col_slots_b.peek();
+            const int grid = slots > 0 && items > slots ? slots : (int)items;
+            col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE_B><<<grid, C::COL_THREADS, C::COL_SMEM_B, st>>>(a);
+            return;
+        }
         const int slots = col_slots.peek();   // set up by every operation before its launches
         const int grid = slots > 0 && items > slots ? slots : (int)items;
-        col_kernel<real, N, C::EC, C::MINB><<<grid, C::COL_THREADS, C::COL_SMEM, st>>>(a);
+        col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE><<<grid, C::COL_THREADS, C::COL_SMEM, st>>>(a);
     }
+    // the row kernel of a grid with nx = N (a.ny / ROWS CTAs per instance)
     static void row(const StageArgs<real>& a, cudaStream_t st) {
         if constexpr (std::is_same<real, float>::value) {
             int slots = 0;
-            if (StepVariant<float>* v = tuned_variant(N, 1, a.ninst > 1, &slots)) {
-                v->launch(a, slots, st);
-                return;
+            if (a.nx == a.ny) {
+                if (StepVariant<float>* v = tuned_variant(N, 1, a.ninst > 1, &slots)) {
+                    v->launch(a, slots, st);
+                    return;
+                }
             }
         }
-        row_kernel<real, N, C::ER, C::ROWS, C::MINB><<<C::ROW_BLOCKS * a.ninst, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
+        row_kernel<real, N, C::ER, C::ROWS, C::MINB><<<(a.ny / C::ROWS) * a.ninst, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
     }
+    // transforms: nx / 2 columns of length N; ny rows of length N
+    static void col_ifft(const cplx<real>* spec, cplx<real>* T, const cplx<real>* tw_y, int nx, cudaStream_t st) {
+        col_ifft_kernel<real, N, C::W, C::EC><<<nx / 2 / C::W, C::COLT_THREADS, C::COLT_SMEM, st>>>(spec, T, tw_y, nx);
+    }
+    static void col_fft(const cplx<real>* T, cplx<real>* spec, const cplx<real>* tw_y, int nx, cudaStream_t st) {
+        col_fft_kernel<real, N, C::W, C::EC><<<nx / 2 / C::W, C::COLT_THREADS, C::COLT_SMEM, st>>>(T, spec, tw_y, nx);
+    }
+    static void row_c2r(const cplx<real>* T, real* phys, const cplx<real>* tw, int ny, cudaStream_t st) {
+        row_c2r_kernel<real, N, C::ERT, C::ROWS_T><<<ny / C::ROWS_T, C::ROWT_THREADS, C::ROWT_SMEM, st>>>(T, phys, tw);
+    }
+    static void row_r2c(const real* phys, cplx<real>* T, const cplx<real>* tw, int ny, cudaStream_t st) {
+        row_r2c_kernel<real, N, C::ERT, C::ROWS_T><<<ny / C::ROWS_T, C::ROWT_THREADS, C::ROWT_SMEM, st>>>(phys, T, tw);
+    }
+    // BwdTrans / FwdTrans of an N x N grid
     static void bwd(const cplx<real>* spec, cplx<real>* T, real* phys, const cplx<real>* tw, cudaStream_t st) {
-        col_ifft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COLT_THREADS, C::COLT_SMEM, st>>>(spec, T, tw);
-        row_c2r_kernel<real, N, C::ERT, C::ROWS_T><<<C::ROWT_BLOCKS, C::ROWT_THREADS, C::ROWT_SMEM, st>>>(T, phys, tw);
+        col_ifft(spec, T, tw, N, st);
+        row_c2r(T, phys, tw, N, st);
     }
     static void fwd(const real* phys, cplx<real>* T, cplx<real>* spec, const cplx<real>* tw, cudaStream_t st) {
-        row_r2c_kernel<real, N, C::ERT, C::ROWS_T><<<C::ROWT_BLOCKS, C::ROWT_THREADS, C::ROWT_SMEM, st>>>(phys, T, tw);
-        col_fft_kernel<real, N, C::W, C::EC><<<C::H / C::W, C::COLT_THREADS, C::COLT_SMEM, st>>>(T, spec, tw);
+        row_r2c(phys, T, tw, N, st);
+        col_fft(T, spec, tw, N, st);
     }
 };
 
-// Calls F::template run<real, N>(args...) for the mesh's precision and size.
+// Calls f(std::integral_constant<int, N>) for a supported transform length N.
+template <class F>
+qaf_status with_n(int N, F&& f) {
+#ifdef QAF_ONLY_N
+    if (N == QAF_ONLY_N) return f(std::integral_constant<int, QAF_ONLY_N>{});
+    return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size (a build for one size only)");
+#endif
+    switch (N) {
+        case 16: return f(std::integral_constant<int, 16>{});
+        case 32: return f(std::integral_constant<int, 32>{});
+        case 64: return f(std::integral_constant<int, 64>{});
+        case 128: return f(std::integral_constant<int, 128>{});
+        case 256: return f(std::integral_constant<int, 256>{});
+        case 512: return f(std::integral_constant<int, 512>{});
+        case 1024: return f(std::integral_constant<int, 1024>{});
+        case 48: return f(std::integral_constant<int, 48>{});
+        case 96: return f(std::integral_constant<int, 96>{});
+        case 192: return f(std::integral_constant<int, 192>{});
+        case 384: return f(std::integral_constant<int, 384>{});
+        case 768: return f(std::integral_constant<int, 768>{});
+        default: return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size");
+    }
+}
+
+// Runtime-size launches on an nx x ny grid: the row kernel and the row
+// transforms are the nx-point kernels, the column ones the ny-point kernels.
+template <typename real>
+qaf_status setup_grid(int nx, int ny) {
+    QAF_TRY(with_n(nx, [](auto n) -> qaf_status { return Launch<real, decltype(n)::value>::setup(); }));
+    if (ny != nx) QAF_TRY(with_n(ny, [](auto n) -> qaf_status { return Launch<real, decltype(n)::value>::setup(); }));
+    return QAF_OK;
+}
+template <typename real>
+void launch_row(const StageArgs<real>& a, cudaStream_t st) {
+    with_n(a.nx, [&](auto n) -> qaf_status { Launch<real, decltype(n)::value>::row(a, st); return QAF_OK; });
+}
+template <typename real>
+void launch_col(const StageArgs<real>& a, cudaStream_t st) {
+    with_n(a.ny, [&](auto n) -> qaf_status { Launch<real, decltype(n)::value>::col(a, st); return QAF_OK; });
+}
+
+// Calls F::template run<real>(args...) for the mesh's precision, after
+// checking that both grid sizes have kernels (the operation's launches take
+// the sizes at run time: launch_row / launch_col, Launch<real, N>::col_*/row_*).
+template <class F, class... A>
+qaf_status dispatch_grid(const qaf_mesh* m, A&&... args) {
+    if (!size_supported(m->desc.nx) || !size_supported(m->desc.ny))
+        return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size (nx and ny each a power of two in "
+                                         "[16, 1024] or 3 * 2^k in [48, 768])");
+#ifdef QAF_ONLY_N
+    if (m->desc.nx != QAF_ONLY_N || m->desc.ny != QAF_ONLY_N)
+        return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size (a build for one size only)");
+#endif
+    return m->desc.dtype == QAF_F64 ? F::template run<double>(std::forward<A>(args)...)
+                                    : F::template run<float>(std::forward<A>(args)...);
+}
+
+// Calls F::template run<real, N>(args...) for the mesh's precision and size
+// (square grids: noalloc step, adjoint).
 template <class F, class... A>
 qaf_status dispatch(const qaf_mesh* m, A&&... args) {
     const int N = m->desc.nx;
+    if (m->desc.ny != N) return fail(QAF_ERR_UNSUPPORTED, "this operation needs nx == ny");
     const bool f64 = m->desc.dtype == QAF_F64;
 #define QAF_CASE(n)                                                                       \
     case n:                                                                               \
@@ -520,24 +644,42 @@ qaf_status post_launch(const char* what) {
 // ---------------------------------------------------------------------------
 // operations
 // ---------------------------------------------------------------------------
+// BwdTrans: the ny-point column inverse transforms of the nx/2 columns, then
+// the nx-point row C2Rs of the ny rows
 struct OpBwd {
-    template <typename real, int N>
+    template <typename real>
     static qaf_status run(qaf_mesh* m, const void* spec, void* phys, cudaStream_t st) {
         QAF_TRY(ensure_ws<real>(m));
-        QAF_TRY((Launch<real, N>::setup()));
+        const int nx = m->desc.nx, ny = m->desc.ny;
+        QAF_TRY(setup_grid<real>(nx, ny));
         Workspace<real>& w = ws<real>(m);
-        Launch<real, N>::bwd(reinterpret_cast<const cplx<real>*>(spec), w.T, reinterpret_cast<real*>(phys), w.tw, st);
+        QAF_TRY(with_n(ny, [&](auto n) -> qaf_status {
+            Launch<real, decltype(n)::value>::col_ifft(reinterpret_cast<const cplx<real>*>(spec), w.T, w.tw_y, nx, st);
+            return QAF_OK;
+        }));
+        QAF_TRY(with_n(nx, [&](auto n) -> qaf_status {
+            Launch<real, decltype(n)::value>::row_c2r(w.T, reinterpret_cast<real*>(phys), w.tw, ny, st);
+            return QAF_OK;
+        }));
         return post_launch("BwdTrans");
     }
 };
 
 struct OpFwd {
-    template <typename real, int N>
+    template <typename real>
     static qaf_status run(qaf_mesh* m, const void* phys, void* spec, cudaStream_t st) {
         QAF_TRY(ensure_ws<real>(m));
-        QAF_TRY((Launch<real, N>::setup()));
+        const int nx = m->desc.nx, ny = m->desc.ny;
+        QAF_TRY(setup_grid<real>(nx, ny));
         Workspace<real>& w = ws<real>(m);
-        Launch<real, N>::fwd(reinterpret_cast<const real*>(phys), w.T, reinterpret_cast<cplx<real>*>(spec), w.tw, st);
+        QAF_TRY(with_n(nx, [&](auto n) -> qaf_status {
+            Launch<real, decltype(n)::value>::row_r2c(reinterpret_cast<const real*>(phys), w.T, w.tw, ny, st);
+            return QAF_OK;
+        }));
+        QAF_TRY(with_n(ny, [&](auto n) -> qaf_status {
+            Launch<real, decltype(n)::value>::col_fft(w.T, reinterpret_cast<cplx<real>*>(spec), w.tw_y, nx, st);
+            return QAF_OK;
+        }));
         return post_launch("FwdTrans");
     }
 };
@@ -545,20 +687,22 @@ struct OpFwd {
 template <typename real>
 void to_internal(qaf_mesh* m, const void* ref, int f, cudaStream_t st) {
     Workspace<real>& w = ws<real>(m);
-    ref_to_internal<real><<<grid_for(spec_elems(m)), 256, 0, st>>>(reinterpret_cast<const cplx<real>*>(ref), w.old_m[f], w.old_n[f], m->desc.nx);
+    ref_to_internal<real><<<grid_for(spec_elems(m)), 256, 0, st>>>(reinterpret_cast<const cplx<real>*>(ref), w.old_m[f], w.old_n[f],
+                                                                    m->desc.nx, m->desc.ny);
 }
 
 template <typename real>
 void from_internal(qaf_mesh* m, cplx<real>* mm, cplx<real>* nq, void* ref, cudaStream_t st) {
-    internal_to_ref<real><<<grid_for(spec_elems(m)), 256, 0, st>>>(mm, nq, reinterpret_cast<cplx<real>*>(ref), m->desc.nx);
+    internal_to_ref<real><<<grid_for(spec_elems(m)), 256, 0, st>>>(mm, nq, reinterpret_cast<cplx<real>*>(ref), m->desc.nx,
+                                                                    m->desc.ny);
 }
 
 struct OpNonlinear {
-    template <typename real, int N>
+    template <typename real>
     static qaf_status run(qaf_mesh* m, const qaf_params* p, const void* const* in, void* const* out, void* phys_out,
                           cudaStream_t st) {
         QAF_TRY(ensure_ws<real>(m));
-        QAF_TRY((Launch<real, N>::setup()));
+        QAF_TRY(setup_grid<real>(m->desc.nx, m->desc.ny));
         Workspace<real>& w = ws<real>(m);
         for (int f = 0; f < 3; ++f) to_internal<real>(m, in[f], f, st);
         m->loaded = true;      // the nonlinear evaluation reuses the state buffers
@@ -569,17 +713,17 @@ struct OpNonlinear {
         a.phys_all = 1;
         a.mode = MODE_PROLOGUE; a.do_inverse = 1;
         QAF_CUDA(cudaMemsetAsync(w.queue, 0, sizeof(int), st));
-        Launch<real, N>::col(a, st);
-        Launch<real, N>::row(a, st);
+        launch_col<real>(a, st);
+        launch_row<real>(a, st);
         a.mode = MODE_NONL; a.do_inverse = 0;
-        Launch<real, N>::col(a, st);
+        launch_col<real>(a, st);
         for (int f = 0; f < 3; ++f) from_internal<real>(m, w.acc_m[f], w.acc_n[f], out[f], st);
         return post_launch("qaf_nonlinear");
     }
 };
 
 struct OpLoad {
-    template <typename real, int N>
+    template <typename real>
     static qaf_status run(qaf_mesh* m, void* const* state, cudaStream_t st) {
         QAF_TRY(ensure_ws<real>(m));
         for (int f = 0; f < 3; ++f) to_internal<real>(m, state[f], f, st);
@@ -591,7 +735,7 @@ struct OpLoad {
 };
 
 struct OpStore {
-    template <typename real, int N>
+    template <typename real>
     static qaf_status run(qaf_mesh* m, void* const* state, cudaStream_t st) {
         Workspace<real>& w = ws<real>(m);
         for (int f = 0; f < 3; ++f) from_internal<real>(m, w.old_m[f], w.old_n[f], state[f], st);
@@ -607,11 +751,11 @@ struct KernelTimer {
 };
 
 struct OpAdvance {
-    template <typename real, int N>
+    template <typename real>
     static qaf_status run(qaf_mesh* m, const qaf_params* p, int integ, int nsteps, bool final_inverse, KernelTimer* timer,
                           cudaStream_t st) {
         QAF_TRY(ensure_ws<real>(m));
-        QAF_TRY((Launch<real, N>::setup()));
+        QAF_TRY(setup_grid<real>(m->desc.nx, m->desc.ny));
         QAF_TRY(ensure_if<real>(m, p, st));
         Workspace<real>& w = ws<real>(m);
         StageArgs<real> a = make_args<real>(m, p);
@@ -623,7 +767,7 @@ struct OpAdvance {
                 cudaEventCreate(&e0); cudaEventCreate(&e1);
                 cudaEventRecord(e0, st);
             }
-            if (kind == 0) Launch<real, N>::row(a, st); else Launch<real, N>::col(a, st);
+            if (kind == 0) launch_row<real>(a, st); else launch_col<real>(a, st);
             if (timer) {
                 cudaEventRecord(e1, st);
                 timer->ev.push_back(e0); timer->ev.push_back(e1); timer->kind.push_back(kind);
@@ -633,7 +777,7 @@ struct OpAdvance {
         if (!m->y_valid) {
             a.mode = MODE_PROLOGUE; a.do_inverse = 1;
             QAF_CUDA(cudaMemsetAsync(w.queue, 0, sizeof(int), st));
-            Launch<real, N>::col(a, st);
+            launch_col<real>(a, st);
             m->launches += 1;
         }
         a.mode = MODE_STAGE;
@@ -770,15 +914,13 @@ qaf_status qaf_mesh_tables(const qaf_mesh* m, void* kx, void* ky, void* k2, void
 qaf_status qaf_bwd_trans(qaf_mesh* m, const void* spec, void* phys, void* stream) {
     QAF_TRY(check_mesh(m));
     if (!spec || !phys) return fail(QAF_ERR_INVALID, "null pointer");
-    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "transforms need nx == ny");
-    return dispatch<OpBwd>(m, m, spec, phys, (cudaStream_t)stream);
+    return dispatch_grid<OpBwd>(m, m, spec, phys, (cudaStream_t)stream);
 }
 
 qaf_status qaf_fwd_trans(qaf_mesh* m, const void* phys, void* spec, void* stream) {
     QAF_TRY(check_mesh(m));
     if (!spec || !phys) return fail(QAF_ERR_INVALID, "null pointer");
-    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "transforms need nx == ny");
-    return dispatch<OpFwd>(m, m, phys, spec, (cudaStream_t)stream);
+    return dispatch_grid<OpFwd>(m, m, phys, spec, (cudaStream_t)stream);
 }
 
 #define QAF_BY_DTYPE(m, KERNEL_F32, KERNEL_F64) \
@@ -881,10 +1023,9 @@ qaf_status qaf_nonlinear_dbg(qaf_mesh* m, const qaf_params* p, const void* w, co
     QAF_TRY(check_mesh(m));
     QAF_TRY(check_params(p));
     if (!w || !r1 || !r2 || !w_nl || !r1_nl || !r2_nl) return fail(QAF_ERR_INVALID, "null pointer");
-    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "the fused path needs nx == ny");
     const void* in[3] = {w, r1, r2};
     void* out[3] = {w_nl, r1_nl, r2_nl};
-    return dispatch<OpNonlinear>(m, m, p, (const void* const*)in, (void* const*)out, phys_out, (cudaStream_t)stream);
+    return dispatch_grid<OpNonlinear>(m, m, p, (const void* const*)in, (void* const*)out, phys_out, (cudaStream_t)stream);
 }
 
 static qaf_status check_advance(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, int nsteps) {
@@ -892,16 +1033,14 @@ static qaf_status check_advance(qaf_mesh* m, const qaf_params* p, qaf_integrator
     QAF_TRY(check_params(p));
     if (integ != QAF_IFE && integ != QAF_IFRK2 && integ != QAF_IFRK4) return fail(QAF_ERR_INVALID, "bad integrator");
     if (nsteps < 0) return fail(QAF_ERR_INVALID, "nsteps < 0");
-    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "the fused path needs nx == ny");
     return QAF_OK;
 }
 
 qaf_status qaf_state_load(qaf_mesh* m, const void* w, const void* r1, const void* r2, void* stream) {
     QAF_TRY(check_mesh(m));
     if (!w || !r1 || !r2) return fail(QAF_ERR_INVALID, "null pointer");
-    if (m->desc.nx != m->desc.ny) return fail(QAF_ERR_UNSUPPORTED, "the fused path needs nx == ny");
     void* st[3] = {const_cast<void*>(w), const_cast<void*>(r1), const_cast<void*>(r2)};
-    return dispatch<OpLoad>(m, m, (void* const*)st, (cudaStream_t)stream);
+    return dispatch_grid<OpLoad>(m, m, (void* const*)st, (cudaStream_t)stream);
 }
 
 qaf_status qaf_state_store(qaf_mesh* m, void* w, void* r1, void* r2, void* stream) {
@@ -909,14 +1048,14 @@ qaf_status qaf_state_store(qaf_mesh* m, void* w, void* r1, void* r2, void* strea
     if (!w || !r1 || !r2) return fail(QAF_ERR_INVALID, "null pointer");
     if (!m->loaded) return fail(QAF_ERR_INVALID, "no state loaded on this mesh");
     void* st[3] = {w, r1, r2};
-    return dispatch<OpStore>(m, m, (void* const*)st, (cudaStream_t)stream);
+    return dispatch_grid<OpStore>(m, m, (void* const*)st, (cudaStream_t)stream);
 }
 
 qaf_status qaf_state_advance(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, int nsteps, void* stream) {
     QAF_TRY(check_advance(m, p, integ, nsteps));
     if (!m->loaded) return fail(QAF_ERR_INVALID, "no state loaded on this mesh");
     if (nsteps == 0) return QAF_OK;
-    return dispatch<OpAdvance>(m, m, p, (int)integ, nsteps, true, (KernelTimer*)nullptr, (cudaStream_t)stream);
+    return dispatch_grid<OpAdvance>(m, m, p, (int)integ, nsteps, true, (KernelTimer*)nullptr, (cudaStream_t)stream);
 }
 
 qaf_status qaf_state_advance_timed(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, int nsteps, double out_ms[3],
@@ -925,7 +1064,7 @@ qaf_status qaf_state_advance_timed(qaf_mesh* m, const qaf_params* p, qaf_integra
     if (!m->loaded) return fail(QAF_ERR_INVALID, "no state loaded on this mesh");
     if (!out_ms) return fail(QAF_ERR_INVALID, "null pointer");
     KernelTimer timer;
-    qaf_status s = nsteps ? dispatch<OpAdvance>(m, m, p, (int)integ, nsteps, true, &timer, (cudaStream_t)stream) : QAF_OK;
+    qaf_status s = nsteps ? dispatch_grid<OpAdvance>(m, m, p, (int)integ, nsteps, true, &timer, (cudaStream_t)stream) : QAF_OK;
     cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
     double sum[2] = {0, 0};
     int cnt[2] = {0, 0};
@@ -960,9 +1099,9 @@ qaf_status qaf_step(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, void
     if (nsteps == 0) return QAF_OK;
     void* st[3] = {w, r1, r2};
     cudaStream_t s = (cudaStream_t)stream;
-    QAF_TRY(dispatch<OpLoad>(m, m, (void* const*)st, s));
-    QAF_TRY(dispatch<OpAdvance>(m, m, p, (int)integ, nsteps, false, (KernelTimer*)nullptr, s));
-    return dispatch<OpStore>(m, m, (void* const*)st, s);
+    QAF_TRY(dispatch_grid<OpLoad>(m, m, (void* const*)st, s));
+    QAF_TRY(dispatch_grid<OpAdvance>(m, m, p, (int)integ, nsteps, false, (KernelTimer*)nullptr, s));
+    return dispatch_grid<OpStore>(m, m, (void* const*)st, s);
 }
 
 qaf_status qaf_step_host(qaf_mesh* m, const qaf_params* p, qaf_integrator integ, void* w, void* r1, void* r2,
@@ -1202,6 +1341,7 @@ size_t noalloc_carve(Workspace<real>& w, cplx<real>* b, int N) {
     w.Ed = b + take((size_t)NE * N);
     w.T = b + take(plane);
     w.tw = b + take(N);
+    w.tw_y = w.tw;
     w.ex = reinterpret_cast<real*>(b + take((4 * (H + 1) + 1) / 2 + 1));
     w.ey = reinterpret_cast<real*>(b + take((4 * N + 1) / 2 + 1));
     w.diag = reinterpret_cast<double*>(b + take(4 * sizeof(double) / sizeof(cplx<real>) + 1));
@@ -1246,7 +1386,7 @@ struct OpStepNoAlloc {
         Workspace<real>& w = ws<real>(m);
         const size_t need = noalloc_carve<real>(w, reinterpret_cast<cplx<real>*>(scratch), N);
         if (need > kNoAllocBytes) return fail(QAF_ERR_INVALID, "qaf_step_noalloc: workspace exceeds the fixed scratch");
-        QAF_TRY(encode_g_map<real>(&w.tm_G, w.G, N));
+        QAF_TRY(encode_g_map<real>(&w.tm_G, w.G, N, N));
         QAF_TRY((Launch<real, N>::setup()));
         noalloc_tables_kernel<real><<<8, 256, 0, st>>>(w.tw, w.ex, w.ey, N, m->dkx, m->dky, p->dt, p->re);
         // the array keeps the previous call's contents: clear the status flags
@@ -1257,7 +1397,7 @@ struct OpStepNoAlloc {
         w.e0[3] = (real)exp(p->q_lin * p->dt * 0.5);
         for (int f = 0; f < 3; ++f)
             ref_to_internal<real><<<grid_for(spec_elems(m)), 256, 0, st>>>(
-                reinterpret_cast<const cplx<real>*>(state[f]), w.old_m[f], w.old_n[f], N);
+                reinterpret_cast<const cplx<real>*>(state[f]), w.old_m[f], w.old_n[f], N, N);
         StageArgs<real> a = make_args<real>(m, p);
         a.integrator = integ;
         const int nst = integ == QAF_IFRK4 ? 4 : (integ == QAF_IFRK2 ? 2 : 1);
@@ -1394,29 +1534,6 @@ template <typename real> std::vector<EnsGroup<real>>& groups(qaf_ensemble* e);
 template <> std::vector<EnsGroup<float>>& groups<float>(qaf_ensemble* e) { return e->gf; }
 template <> std::vector<EnsGroup<double>>& groups<double>(qaf_ensemble* e) { return e->gd; }
 
-// call f(std::integral_constant<int, N>) for a supported N
-template <class F>
-qaf_status with_n(int N, F&& f) {
-#ifdef QAF_ONLY_N
-    if (N == QAF_ONLY_N) return f(std::integral_constant<int, QAF_ONLY_N>{});
-    return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size (a build for one size only)");
-#endif
-    switch (N) {
-        case 16: return f(std::integral_constant<int, 16>{});
-        case 32: return f(std::integral_constant<int, 32>{});
-        case 64: return f(std::integral_constant<int, 64>{});
-        case 128: return f(std::integral_constant<int, 128>{});
-        case 256: return f(std::integral_constant<int, 256>{});
-        case 512: return f(std::integral_constant<int, 512>{});
-        case 1024: return f(std::integral_constant<int, 1024>{});
-        case 48: return f(std::integral_constant<int, 48>{});
-        case 96: return f(std::integral_constant<int, 96>{});
-        case 192: return f(std::integral_constant<int, 192>{});
-        case 384: return f(std::integral_constant<int, 384>{});
-        case 768: return f(std::integral_constant<int, 768>{});
-        default: return fail(QAF_ERR_UNSUPPORTED, "no kernels for this grid size");
-    }
-}
 
 template <typename real>
 StageArgs<real> group_args(const qaf_ensemble* e, const EnsGroup<real>& g) {
@@ -1426,12 +1543,13 @@ StageArgs<real> group_args(const qaf_ensemble* e, const EnsGroup<real>& g) {
     a.dkx = (real)(2 * M_PI / e->lx); a.dky = (real)(2 * M_PI / e->ly);
     a.lambda = (real)e->p.lambda; a.ce = (real)(1.0 / (e->p.er * e->p.re)); a.alpha = (real)e->p.alpha;
     a.dt = (real)e->p.dt; a.advect = e->p.advect_omega ? 1 : 0;
-    set_mask(a, N, e->p.no_dealias);
+    a.nx = N; a.ny = N;
+    set_mask(a, N, N, e->p.no_dealias);
     for (int f = 0; f < 3; ++f) {
         a.old_m[f] = g.w.old_m[f]; a.old_n[f] = g.w.old_n[f]; a.acc_m[f] = g.w.acc_m[f]; a.acc_n[f] = g.w.acc_n[f];
         a.nl_m[f] = g.w.acc_m[f]; a.nl_n[f] = g.w.acc_n[f];
     }
-    a.Y = g.w.Y; a.D = g.w.D; a.G = g.w.G; a.Ed = g.w.Ed; a.tw = g.w.tw; a.ex = g.w.ex; a.ey = g.w.ey;
+    a.Y = g.w.Y; a.D = g.w.D; a.G = g.w.G; a.Ed = g.w.Ed; a.tw = g.w.tw; a.tw_y = g.w.tw; a.ex = g.w.ex; a.ey = g.w.ey;
     a.flags = g.w.flags; a.queue = g.w.queue; a.tm_G = g.w.tm_G;
     a.ninst = g.ninst; a.istride = g.istride;
     a.inst_alpha = g.inst_alpha; a.inst_e0 = g.inst_e0;
@@ -1482,7 +1600,7 @@ qaf_status build_groups(qaf_ensemble* e, const double* alpha, const double* rf) 
         // host-built tables, the same as a single mesh's
         const std::vector<cplx<real>> tw = host_twiddles<real>(N);
         std::vector<real> ex, ey, ia(g.ninst), ie0(4 * (size_t)g.ninst);
-        host_if_tables<real>(N, 2 * M_PI / e->lx, 2 * M_PI / e->ly, e->p.dt, e->p.re, ex, ey);
+        host_if_tables<real>(N, N, 2 * M_PI / e->lx, 2 * M_PI / e->ly, e->p.dt, e->p.re, ex, ey);
         for (int s2 = 0; s2 < g.ninst; ++s2) {
             const int k = g.members[s2];
             ia[s2] = (real)alpha[k];
@@ -1496,7 +1614,7 @@ qaf_status build_groups(qaf_ensemble* e, const double* alpha, const double* rf) 
         QAF_CUDA(cudaMemset(g.w.flags, 0, 16));
         QAF_CUDA(cudaMemset(g.diag, 0, 2 * (size_t)g.ninst * sizeof(double)));
         // TMA view of every instance's G arrays
-        QAF_TRY(encode_g_map<real>(&g.w.tm_G, g.w.G, N, (size_t)(g.ninst - 1) * (g.istride / H) + (size_t)NG * N));
+        QAF_TRY(encode_g_map<real>(&g.w.tm_G, g.w.G, N, N, (size_t)(g.ninst - 1) * (g.istride / H) + (size_t)NG * N));
         qaf_status st = with_n(N, [&](auto n) -> qaf_status { return Launch<real, decltype(n)::value>::setup(); });
         if (st != QAF_OK) return st;
         G.push_back(g);
@@ -1566,10 +1684,10 @@ qaf_status ens_copy(qaf_ensemble* e, int inst, void* const* st3, bool load, cuda
     for (int f = 0; f < 3; ++f) {
         if (load)
             ref_to_internal<real><<<grid_for(n), 256, 0, st>>>(reinterpret_cast<const cplx<real>*>(st3[f]),
-                                                             g.w.old_m[f] + io, g.w.old_n[f] + io, g.N);
+                                                             g.w.old_m[f] + io, g.w.old_n[f] + io, g.N, g.N);
         else
             internal_to_ref<real><<<grid_for(n), 256, 0, st>>>(g.w.old_m[f] + io, g.w.old_n[f] + io,
-                                                             reinterpret_cast<cplx<real>*>(st3[f]), g.N);
+                                                             reinterpret_cast<cplx<real>*>(st3[f]), g.N, g.N);
     }
     if (load) e->y_valid = false;
     return post_launch(load ? "qaf_ensemble_load" : "qaf_ensemble_store");
@@ -1855,7 +1973,7 @@ struct OpAdjForward {
         const size_t ns = A->ns, cb = sizeof(cplx<real>);
         for (int f = 0; f < 3; ++f)
             QAF_CUDA(cudaMemcpyAsync(adj_field<real>(A->ckpt, ns, f), s0[f], ns * cb, cudaMemcpyDeviceToDevice, st));
-        QAF_TRY((OpLoad::run<real, N>(m, const_cast<void* const*>(s0), st)));
+        QAF_TRY((OpLoad::run<real>(m, const_cast<void* const*>(s0), st)));
         QAF_CUDA(cudaMemsetAsync(A->loss, 0, sizeof(double), st));
         const double n4 = (double)N * N * (double)N * N;
         for (int seg = 0; seg < A->nseg; ++seg) {
@@ -1866,10 +1984,10 @@ struct OpAdjForward {
             if (t1 < A->nsteps) {
                 unsigned char* c = A->ckpt + (size_t)(seg + 1) * 3 * ns * cb;
                 void* dst[3] = {adj_field<real>(c, ns, 0), adj_field<real>(c, ns, 1), adj_field<real>(c, ns, 2)};
-                QAF_TRY((OpStore::run<real, N>(m, dst, st)));
+                QAF_TRY((OpStore::run<real>(m, dst, st)));
             }
         }
-        if (sT[0] && sT[1] && sT[2]) QAF_TRY((OpStore::run<real, N>(m, sT, st)));
+        if (sT[0] && sT[1] && sT[2]) QAF_TRY((OpStore::run<real>(m, sT, st)));
         double h = 0;
         QAF_CUDA(cudaMemcpyAsync(&h, A->loss, sizeof(double), cudaMemcpyDeviceToHost, st));
         QAF_CUDA(cudaStreamSynchronize(st));
@@ -1921,7 +2039,7 @@ struct OpAdjBackward {
         a.dkx = (real)m->dkx; a.dky = (real)m->dky; a.dt = (real)A->p.dt; a.lambda = (real)A->p.lambda;
         a.ce = (real)(1.0 / (A->p.er * A->p.re));
         a.advect = A->p.advect_omega ? 1 : 0;
-        set_mask(a, N, A->p.no_dealias);
+        set_mask(a, N, N, A->p.no_dealias);
         a.tw = w.tw; a.ex = w.ex; a.ey = w.ey;
         for (int c = 0; c < 4; ++c) a.e0[c] = w.e0[c];
         a.Tg = reinterpret_cast<cplx<real>*>(A->Tg); a.Tx = reinterpret_cast<cplx<real>*>(A->Tx);
@@ -1955,7 +2073,7 @@ struct OpAdjBackward {
             const int t0 = seg * A->K, t1 = std::min(T, t0 + A->K);
             unsigned char* c = A->ckpt + (size_t)seg * 3 * ns * cb;
             const void* cs[3] = {adj_field<real>(c, ns, 0), adj_field<real>(c, ns, 1), adj_field<real>(c, ns, 2)};
-            QAF_TRY((OpLoad::run<real, N>(m, const_cast<void* const*>(cs), st)));
+            QAF_TRY((OpLoad::run<real>(m, const_cast<void* const*>(cs), st)));
             AdjRecord rec{A->phys, A->wlog, nullptr, 0, 0.0};
             QAF_TRY((OpRecord::run<real, N>(m, &A->p, t1 - t0, &rec, st)));
             auto w_at = [&](int n) -> const cplx<real>* {   // w of the state at time n (t0 <= n <= t1)
@@ -2493,7 +2611,7 @@ qaf_status batch_backward(qaf_adjoint_batch* B, const void* const* gT, const dou
     a.dkx = (real)(2 * M_PI / e->lx); a.dky = (real)(2 * M_PI / e->ly); a.dt = (real)p.dt; a.lambda = (real)p.lambda;
     a.ce = (real)(1.0 / (p.er * p.re));
     a.advect = p.advect_omega ? 1 : 0;
-    set_mask(a, N, p.no_dealias);
+    set_mask(a, N, N, p.no_dealias);
     a.tw = g.w.tw; a.ex = g.w.ex; a.ey = g.w.ey;
     host_if_e0<real>(p.dt, p.re, p.rf, p.q_lin, a.e0);
     a.Tg = reinterpret_cast<cplx<real>*>(B->Tg); a.Tx = reinterpret_cast<cplx<real>*>(B->Tx);

@@ -218,7 +218,9 @@ struct TwLayout {
     static constexpr int count = Sc::passes > 1 ? offset(Sc::passes) : 0;
 };
 
-template <typename real, int L, int E, bool INV, int P>
+// base: the thread's twiddle bases, base index i at base[i * BS] (BS = 1:
+// a register array; BS = TEAM: a shared table [i][t] read at &table[t])
+template <typename real, int L, int E, bool INV, int P, int BS = 1>
 QAF_HD void stockham_pass_tw(int t, cplx<real>* v, const cplx<real>* base) {
     using Sc = Sched<L, E>;
     constexpr int R = Sc::radix(P), NB = E / R;
@@ -228,7 +230,7 @@ QAF_HD void stockham_pass_tw(int t, cplx<real>* v, const cplx<real>* base) {
 #pragma unroll
         for (int q = 0; q < R; ++q) x[q] = v[s + q * NB];
         if constexpr (P > 0) {
-            cplx<real> w = base[TwLayout<L, E>::offset(P) + s];
+            cplx<real> w = base[(TwLayout<L, E>::offset(P) + s) * BS];
             if (INV) w.y = -w.y;
             cplx<real> wq = w;
 #pragma unroll
@@ -286,6 +288,82 @@ struct TeamFFT {
             for (int e = 0; e < E; ++e) v[e] = xchg.read(t + TEAM * e);
             xchg.sync();
             pass<INV, P + 1, X>(t, v, xchg);
+        }
+    }
+};
+
+// The same transform with the twiddle bases in a shared-memory table
+// [base index][t] (NBASE * TEAM entries) instead of registers: the table is
+// filled once per CTA (fill: one thread per t computes its bases as
+// TeamFFT::init does and stores them), teams of several columns share it,
+// and a pass reads the thread's bases with consecutive-t (conflict-free,
+// broadcast across the teams of a warp) loads. Frees the registers the
+// bases would hold for the rest of the kernel's state.
+template <typename real, int L, int E>
+struct TeamFFTShared {
+    using Sc = Sched<L, E>;
+    static constexpr int TEAM = L / E;
+    static constexpr int NBASE = TwLayout<L, E>::count;
+    static constexpr int ENTRIES = (NBASE > 0 ? NBASE : 1) * TEAM;
+    const cplx<real>* tab;   // &table[t] of the calling thread
+
+    template <int TWN>
+    __device__ static void fill(cplx<real>* table, int t, const cplx<real>* tw) {
+        TeamFFT<real, L, E> f;
+        f.template init<TWN>(t, tw);
+#pragma unroll
+        for (int i = 0; i < NBASE; ++i) table[i * TEAM + t] = f.base[i];
+    }
+    template <bool INV, class X>
+    __device__ void run(int t, cplx<real>* v, X& xchg) const {
+        pass<INV, 0, X>(t, v, xchg);
+    }
+    template <bool INV, int P, class X>
+    __device__ void pass(int t, cplx<real>* v, X& xchg) const {
+        constexpr int R = Sc::radix(P), S = Sc::span(P);
+        stockham_pass_tw<real, L, E, INV, P, TEAM>(t, v, tab);
+        if constexpr (P + 1 < Sc::passes) {
+#pragma unroll
+            for (int slot = 0; slot < E; ++slot) xchg.write(stockham_dest<L, E, R, S>(t, slot), v[slot]);
+            xchg.sync();
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = xchg.read(t + TEAM * e);
+            xchg.sync();
+            pass<INV, P + 1, X>(t, v, xchg);
+        }
+    }
+
+    // The transform with a double-buffered exchange between interleaved
+    // column teams (element idx of team w at buf[idx * W + w]): pass P's
+    // outputs go to `ext` (P even) or to `in` (P odd), one barrier per
+    // exchange. `in` holds the input the threads loaded before the first
+    // pass, so it is free for writing once the first exchange's barrier has
+    // passed; an odd number of exchanges ends with a barrier, so that `ext`
+    // is free for the next call when this one returns.
+    // SWZ (E a multiple of 4): element idx at idx ^ ((idx / E) & 3), which
+    // spreads the first pass's stores E t + r of neighbouring t over the banks
+    template <bool INV, bool SWZ = false>
+    __device__ void run_db(int t, cplx<real>* v, cplx<real>* ext, cplx<real>* in, int w, int W) const {
+        pass_db<INV, SWZ, 0>(t, v, ext, in, w, W);
+        if constexpr ((Sc::passes - 1) % 2 == 1) __syncthreads();
+    }
+    template <bool SWZ>
+    __device__ static int at(int idx) {
+        if constexpr (SWZ) return idx ^ ((idx / E) & 3);
+        else return idx;
+    }
+    template <bool INV, bool SWZ, int P>
+    __device__ void pass_db(int t, cplx<real>* v, cplx<real>* ext, cplx<real>* in, int w, int W) const {
+        constexpr int R = Sc::radix(P), S = Sc::span(P);
+        stockham_pass_tw<real, L, E, INV, P, TEAM>(t, v, tab);
+        if constexpr (P + 1 < Sc::passes) {
+            cplx<real>* b = (P % 2 == 0) ? ext : in;
+#pragma unroll
+            for (int slot = 0; slot < E; ++slot) b[at<SWZ>(stockham_dest<L, E, R, S>(t, slot)) * W + w] = v[slot];
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = b[at<SWZ>(t + TEAM * e) * W + w];
+            pass_db<INV, SWZ, P + 1>(t, v, ext, in, w, W);
         }
     }
 };

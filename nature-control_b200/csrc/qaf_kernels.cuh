@@ -4,6 +4,8 @@
 
 #include "qaf_stage.cuh"
 
+#include <type_traits>
+
 namespace qaf {
 
 // Select one of three pointers without indexing the kernel-parameter array
@@ -67,7 +69,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsign
 // Column kernel (persistent). Work items, largest first:
 //   [0, TILES)            the r1 and r2 columns of tile T (4 + 4 y-FFTs)
 //   [TILES, 2 TILES)      the w columns of tile T (3 + 4 y-FFTs)
-//   [2 TILES, 2 TILES+3)  the kx = 0 / kx = N/2 edge columns of field f
+//   [2 TILES, 2 TILES+3)  the kx = 0 / kx = nx/2 edge columns of field f
+// (TILES = nx / 2 / TW)
 // A tile is TW kx-columns over all N rows, one contiguous slab of each array.
 // Every slab an item reads (G arrays, old, acc) is fetched by one TMA bulk
 // copy into a ring of three shared-memory buffers, issued up to three slabs
@@ -81,11 +84,29 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsign
 // in flight before it exits. The other CTAs take the remaining items; the
 // host sees FLAG_WAIT_TIMEOUT.
 // ---------------------------------------------------------------------------
-template <typename real, int N, int E>
+// MODE 0: twiddle bases in registers; the item code inlined whole for FP64 at
+// N >= 512 only. MODE 1: twiddle bases in a shared table (TeamFFTShared) and
+// the item code always inlined, so no array is passed by reference through a
+// call frame (local memory, which the shared-memory carve-out leaves little
+// L1 for). MODE 2: MODE 1 plus a fourth slab-sized buffer that makes every
+// y-FFT exchange double-buffered (one barrier per exchange instead of two)
+// and the integrating factors' ky table in shared memory (for launches of
+// one CTA per SM, which leave the room); MODE 3 / 4: MODE 2 with a copy ring
+// of 4 / 5 slabs. +16: the double-buffered exchange swizzled (XOR of an
+// index's low two bits with bits of idx / E).
+//
+// N is the column length ny (the y-transforms' length); the number of
+// kx-columns H = nx / 2, and with it the tiles and work items, is a launch
+// argument.
+template <typename real, int N, int E, int MODE = 0>
 struct ColKernel {
-    static constexpr int H = N / 2, TEAM = N / E, TILES = H / TW, NTHREADS = TW * TEAM;
-    static constexpr int NITEMS = 2 * TILES + 3;
+    static constexpr int TEAM = N / E, NTHREADS = TW * TEAM;
     static constexpr size_t SLAB = (size_t)N * TW;   // complex elements of one slab
+    static constexpr int BASE = MODE & 15;
+    static constexpr bool SB = BASE >= 1;            // shared twiddle bases
+    static constexpr bool DB = BASE >= 2;            // double-buffered exchange, ky factors in shared memory
+    static constexpr int NBUF = BASE == 3 ? 4 : (BASE >= 4 ? 5 : 3);   // slab buffers in the copy ring
+    static constexpr bool SWZ = DB && (MODE & 16) && E % 4 == 0;
     // elements whose IF factors are fetched ahead of the stage-update stores;
     // at 1024^2 the extra live registers cost more in spills than they save
     static constexpr int PF = N >= 1024 ? 1 : (E < 4 ? E : 4);
@@ -93,7 +114,7 @@ struct ColKernel {
     // state stays in registers rather than in the call frame (measured 9%
     // faster at 1024^2; slower for FP32 and smaller FP64 grids, which keep
     // the compiler's own choice)
-    static constexpr bool INLINE_ITEM = sizeof(real) == 8 && N >= 512;
+    static constexpr bool INLINE_ITEM = SB || (sizeof(real) == 8 && N >= 512);
     // the diagnostics' per-warp sums meet in shared memory and leave with one
     // pair of atomics per CTA, except in the FP32 1024^2 kernel, where the
     // extra barrier measured slower than the per-warp atomics
@@ -105,13 +126,22 @@ struct ColKernel {
     }
     static constexpr int BOXR = g_box_rows(N);         // rows per TMA box (at most 256, divides N)
     static_assert(N % BOXR == 0 && BOXR <= 256, "TMA boxes tile a slab");
-    static constexpr size_t SMEM = 3 * SLAB * sizeof(cplx<real>) + 2 * N * sizeof(cplx<real>) + 4 * sizeof(uint64_t) + 16;
-    using FFT = TeamFFT<real, N, E>;
+    using FFT = std::conditional_t<SB, TeamFFTShared<real, N, E>, TeamFFT<real, N, E>>;
+    // MODE 0: slabs | edge table (2N) | mbarriers | ints;
+    // MODE 1: slabs | twiddle table | 64 doubles of diagnostic sums | mbarriers | ints
+    // (the edge table then lives in slab 1: edge items run with no copy in flight)
+    // MODE 2: slabs | extra exchange slab | twiddle table | ky factors (4N) | 64 doubles | mbarriers | ints
+    static constexpr size_t SMEM = SB ? (NBUF + (DB ? 1 : 0)) * SLAB * sizeof(cplx<real>) +
+                                            TeamFFTShared<real, N, E>::ENTRIES * sizeof(cplx<real>) +
+                                            (DB ? 4 * N * sizeof(real) : 0) + 64 * sizeof(double) +
+                                            (NBUF + 1) * sizeof(uint64_t) + 16
+                                      : 3 * SLAB * sizeof(cplx<real>) + 2 * N * sizeof(cplx<real>) + 4 * sizeof(uint64_t) + 16;
     using X = XchgCols<real>;   // exchange layout of the tile's y-FFTs
 
     const StageArgs<real>& a;
     const FFT& fft;
     int t, w;
+    int H;                 // kx-columns nx / 2 (the last, kx = H, is an edge column)
     cplx<real>* bufs;      // three slab buffers back to back
     uint64_t* mbar;        // one mbarrier per buffer
     volatile int* aborted; // shared: a wait of this CTA ran out
@@ -125,7 +155,9 @@ struct ColKernel {
     double* red;           // per-warp diagnostic partial sums (the edge table's space, unused by tiles)
     int q_cur;             // queue index of the current item (test hook)
     unsigned armed;        // thread 0: bit b, parity of buffer b's latest armed phase
-    unsigned withheld;     // thread 0: the buffer of the test hook's withheld copy (3: none)
+    cplx<real>* xbuf;      // MODE 2: the extra exchange buffer
+    const real* eys;       // MODE 2: the ky factors ey[4][N] in shared memory
+    unsigned withheld;     // thread 0: the buffer of the test hook's withheld copy (NBUF: none)
 
     __device__ cplx<real>* buf(int b) const { return bufs + (size_t)b * SLAB; }
     __device__ int nG(int f) const { return a.mode == MODE_PROLOGUE ? 0 : (f == 0 ? 3 : 2); }
@@ -149,7 +181,7 @@ struct ColKernel {
     __device__ void issue_upto(int k) {
         if (k > nseq) k = nseq;
         while (next < k) {
-            const int b = next % 3;
+            const int b = next % NBUF;
             __syncthreads();   // every thread is done with buffer b
             // an aborted CTA arms nothing more: thread 0 sees the mark once its
             // own wait for buffer b's previous slab gave up or was skipped, so
@@ -169,7 +201,7 @@ struct ColKernel {
 #pragma unroll 1
                     for (int r0 = 0; r0 < N; r0 += BOXR)
                         tile_load_2d(buf(b) + (size_t)r0 * TW, &a.tm_G, T * TW * CPE,
-                                     (int)((io / H) + (size_t)g * N + r0), &mbar[b]);
+                                     (int)((io / (size_t)H) + (size_t)g * N + r0), &mbar[b]);
                 } else {
                     bulk_load(buf(b), slab_state(next), bytes, &mbar[b]);
                 }
@@ -181,7 +213,7 @@ struct ColKernel {
     // the test hook's slab of item 0
     __device__ bool dropped(int sidx) const { return a.drop_slab == sidx + 1 && q_cur == 0; }
     __device__ cplx<real>* wait(int sidx) {
-        const int b = sidx % 3;
+        const int b = sidx % NBUF;
         // the default poll limit, or the test's lower one for the copy it withheld
         const unsigned polls = dropped(sidx) ? a.wait_polls : 0u;
         if (!*aborted && !mbar_wait(&mbar[b], ((parity >> b) & 1u) ^ 1u, a.flags, polls)) *aborted = 1;
@@ -193,26 +225,30 @@ struct ColKernel {
     // phase whose copy never came runs out once more
     __device__ void drain() {
         if (threadIdx.x == 0)
-            for (int b = 0; b < 3; ++b)
+            for (int b = 0; b < NBUF; ++b)
                 mbar_wait(&mbar[b], ((armed >> b) & 1u) ^ 1u, nullptr, b == (int)withheld ? a.wait_polls : 0u);
     }
 
     // forward y-FFT of slab sidx; adds ky^pow * F_y(G) to nl
     __device__ void forward(int sidx, int pow, cplx<real> (&nl)[E]) {
         cplx<real>* b = wait(sidx);
-        X x{b, w, TW};
         cplx<real> v[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) v[e] = b[(t + TEAM * e) * TW + w];
-        x.sync();
-        fft.template run<false>(t, v, x);
+        if constexpr (DB) {
+            fft.template run_db<false, SWZ>(t, v, xbuf, b, w, TW);
+        } else {
+            X x{b, w, TW};
+            x.sync();
+            fft.template run<false>(t, v, x);
+        }
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const real ky = ky_of<real>(t + TEAM * e, N, a.dky);
             const real m = pow == 0 ? (real)1 : (pow == 1 ? ky : ky * ky);
             nl[e] = cadd(nl[e], cscale(v[e], m));
         }
-        issue_upto(sidx + 4);
+        issue_upto(sidx + NBUF + 1);
     }
 
     // field f of the current tile; its slabs start at s0
@@ -221,7 +257,7 @@ struct ColKernel {
         const int i = T * TW + w;
         const bool edge_col = (i == 0);   // kx = 0 belongs to the edge item
         const real kx = a.dkx * (real)i;
-        const real sc = (real)1 / ((real)N * (real)N);
+        const real sc = (real)1 / ((real)a.nx * (real)a.ny);
         const int ng = nG(f);
         const size_t base = io + (size_t)T * SLAB;
         cplx<real> nl[E], curr[E];
@@ -263,8 +299,13 @@ struct ColKernel {
 #pragma unroll
                 for (int c = 0; c < PF; ++c) {
                     const int j = t + TEAM * (c0 + c);
-                    Efs[c] = exf * table(&a.ey[cls * N + j]);
-                    Ehs[c] = exh * table(&a.ey[(cls + 1) * N + j]);
+                    if constexpr (DB) {
+                        Efs[c] = exf * eys[cls * N + j];
+                        Ehs[c] = exh * eys[(cls + 1) * N + j];
+                    } else {
+                        Efs[c] = exf * table(&a.ey[cls * N + j]);
+                        Ehs[c] = exh * table(&a.ey[(cls + 1) * N + j]);
+                    }
                 }
 #pragma unroll
                 for (int c = 0; c < PF; ++c) {
@@ -330,10 +371,12 @@ struct ColKernel {
         // the buffer of the last state slab hosts the inverse transforms; the
         // other one is free now
         const int sx = need_acc ? sa : so;
-        if (need_old && need_acc) issue_upto(so + 4);
-        if (!a.do_inverse) { issue_upto(sx + 4); return; }
-        X x{buf(sx % 3), w, TW};
-        x.sync();   // every thread has read its old/acc values
+        if (need_old && need_acc) issue_upto(so + NBUF + 1);
+        if (!a.do_inverse) { issue_upto(sx + NBUF + 1); return; }
+        X x{buf(sx % NBUF), w, TW};
+        // every thread has read its old/acc values (MODE 2: the first
+        // exchange writes the extra buffer, and its barrier comes first)
+        if constexpr (!DB) x.sync();
         const int nq = f == 0 ? 4 : 2;
         for (int qq = 0; qq < nq; ++qq) {
             const int q = f == 0 ? (qq == 0 ? 0 : qq + 2) : (f == 1 ? (qq == 0 ? 1 : 6) : (qq == 0 ? 2 : 7));
@@ -343,13 +386,14 @@ struct ColKernel {
                 const real ky = ky_of<real>(t + TEAM * e, N, a.dky);
                 v[e] = y_mult<real>(q, curr[e], ky, kx * kx + ky * ky, sc);
             }
-            fft.template run<true>(t, v, x);
+            if constexpr (DB) fft.template run_db<true, SWZ>(t, v, xbuf, buf(sx % NBUF), w, TW);
+            else fft.template run<true>(t, v, x);
             cplx<real>* Y = a.Y + io + (size_t)q * N * H + i;
 #pragma unroll
             for (int e = 0; e < E; ++e) Y[(size_t)(t + TEAM * e) * H] = v[e];
-            x.sync();   // the next transform reuses the buffer
+            if constexpr (!DB) x.sync();   // the next transform reuses the buffer
         }
-        issue_upto(sx + 4);
+        issue_upto(sx + NBUF + 1);
     }
 
     // a regular item: the fields fa_ (and fb_ >= 0) of tile T_ of instance inst_
@@ -366,7 +410,7 @@ struct ColKernel {
         per_a = per_field(fa);
         nseq = per_a + (fb >= 0 ? per_field(fb) : 0);
         next = 0;
-        issue_upto(3);
+        issue_upto(NBUF);
         if constexpr (INLINE_ITEM) {
             field_body(fa, 0);
             if (fb >= 0) field_body(fb, per_a);
@@ -406,12 +450,13 @@ template <typename real, int N, int W, int E>
 __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int inst, int t, int w, cplx<real>* buf,
                                          cplx<real>* ctab) {
     const size_t io = (size_t)inst * a.istride;
-    constexpr int H = N / 2, TEAM = N / E;
+    constexpr int TEAM = N / E;
+    const int H = a.nx / 2;   // the kx = nx/2 column
     XchgCols<real> x{buf, w, W};
     TeamFFT<real, N, E> fft;
-    fft.template init<N>(t, a.tw);
+    fft.template init<N>(t, a.tw_y);
     const real kN = a.dkx * (real)H;
-    const real s = (real)1 / ((real)N * (real)N);
+    const real s = (real)1 / ((real)a.nx * (real)a.ny);
     cplx<real> v[E];
     // N^ of columns kx = 0 (ctab[j]) and kx = N/2 (ctab[N + j]), summed over
     // the products in shared memory; team 0 owns every j of a column
@@ -598,31 +643,55 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int in
     }
 }
 
-template <typename real, int N, int E, int MINB>
+template <typename real, int N, int E, int MINB, int MODE = 0>
 __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_constant__ StageArgs<real> a) {
-    using K = ColKernel<real, N, E>;
+    using K = ColKernel<real, N, E, MODE>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<real>* bufs = reinterpret_cast<cplx<real>*>(smem_raw);
-    cplx<real>* ctab = bufs + 3 * K::SLAB;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(ctab + 2 * N);
-    int* item_sh = reinterpret_cast<int*>(mbar + 3);
-    volatile int* aborted = item_sh + 1;
     const int tid = threadIdx.x, w = tid % TW, t = tid / TW;
+    cplx<real>* ctab;
+    double* red;
+    uint64_t* mbar;
+    typename K::FFT fft;
+    cplx<real>* xbuf = nullptr;
+    real* eys = nullptr;
+    if constexpr (K::SB) {
+        cplx<real>* table = bufs + (K::NBUF + (K::DB ? 1 : 0)) * K::SLAB;
+        if constexpr (K::DB) {
+            xbuf = bufs + K::NBUF * K::SLAB;
+            eys = reinterpret_cast<real*>(table + K::FFT::ENTRIES);
+            for (int k = tid; k < 4 * N; k += blockDim.x) eys[k] = a.ey[k];
+        }
+        ctab = bufs + K::SLAB;
+        red = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(table + K::FFT::ENTRIES) +
+                                        (K::DB ? 4 * N * sizeof(real) : 0));
+        mbar = reinterpret_cast<uint64_t*>(red + 64);
+        if (w == 0) K::FFT::template fill<N>(table, t, a.tw_y);
+        fft.tab = table + t;
+    } else {
+        ctab = bufs + 3 * K::SLAB;
+        red = reinterpret_cast<double*>(ctab);
+        mbar = reinterpret_cast<uint64_t*>(ctab + 2 * N);
+        fft.template init<N>(t, a.tw_y);
+    }
+    int* item_sh = reinterpret_cast<int*>(mbar + K::NBUF);
+    volatile int* aborted = item_sh + 1;
     if (tid == 0) {
-        for (int b = 0; b < 3; ++b) mbar_init(&mbar[b], 1);
+        for (int b = 0; b < K::NBUF; ++b) mbar_init(&mbar[b], 1);
         *aborted = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
-    typename K::FFT fft;
-    fft.template init<N>(t, a.tw);
-    K k{a, fft, t, w, bufs, mbar, aborted, 0u, 0, 0, 0, 0, 0, 0, false, false};
-    k.red = reinterpret_cast<double*>(ctab);
+    __syncthreads();   // barriers initialised, twiddle table filled
+    K k{a, fft, t, w, a.nx / 2, bufs, mbar, aborted, 0u, 0, 0, 0, 0, 0, 0, false, false};
+    k.red = red;
+    k.xbuf = xbuf;
+    k.eys = eys;
     k.armed = 0u;
-    k.withheld = 3u;
+    k.withheld = (unsigned)K::NBUF;
     // item q of the launch: kind-major over instances (all r1+r2 tiles of all
     // instances first, then the w tiles, then the edge columns)
-    const int total = K::NITEMS * a.ninst;
+    const int tiles = k.H / TW;
+    const int total = (2 * tiles + 3) * a.ninst;
     for (;;) {
         if (tid == 0) *item_sh = atomicAdd(a.queue, 1);
         __syncthreads();
@@ -636,21 +705,22 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
         if (q >= total) break;
         k.q_cur = q;
         const int local = q / a.ninst, inst = q % a.ninst;
-        if (local < K::TILES) {
+        if (local < tiles) {
             if constexpr (K::INLINE_ITEM) k.item_body(1, 2, local, inst);
             else k.item(1, 2, local, inst);
-        } else if (local < 2 * K::TILES) {
-            if constexpr (K::INLINE_ITEM) k.item_body(0, -1, local - K::TILES, inst);
-            else k.item(0, -1, local - K::TILES, inst);
+        } else if (local < 2 * tiles) {
+            if constexpr (K::INLINE_ITEM) k.item_body(0, -1, local - tiles, inst);
+            else k.item(0, -1, local - tiles, inst);
         } else {
-            col_edge<real, N, TW, E>(a, local - 2 * K::TILES, inst, t, w, bufs, ctab);
+            col_edge<real, N, TW, E>(a, local - 2 * tiles, inst, t, w, bufs, ctab);
             __syncthreads();
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// Row kernel: ROWS rows per CTA, a team of N/E threads per row.
+// Row kernel: ROWS rows per CTA, a team of N/E threads per row. N is the row
+// length nx; the number of rows, ny, is a launch argument (ROWS divides it).
 //
 // Real transforms are done two at a time as one length-N complex FFT:
 //   C2R pair (a, b):  z = IFFT_N(A + i B) = a + i b, with A, B the Hermitian
@@ -676,15 +746,19 @@ struct XchgTeam {
     }
 };
 
-template <typename real, int N, int E, int ROWS>
+// MODE 1: the twiddle bases in a shared table after the rows' regions
+// (TeamFFTShared), shared by the CTA's row teams
+template <typename real, int N, int E, int ROWS, int MODE = 0>
 struct RowKernel {
     static constexpr int H = N / 2, TEAM = N / E, PH = E / 2;
+    static constexpr bool SB = MODE >= 1;
+    using FFT = std::conditional_t<SB, TeamFFTShared<real, N, E>, TeamFFT<real, N, E>>;
     // a named barrier per row team when teams are whole warps and there is more than one team
     static constexpr bool NAMED = (TEAM % 32 == 0) && ROWS > 1 && ROWS <= 15;
     using X = XchgTeam<real, TEAM, NAMED>;
     static constexpr int NKEEP = 5;   // r1, r2, w, two scratch products
     static constexpr size_t SMEM_PER_ROW = N * sizeof(cplx<real>) + NKEEP * N * sizeof(real);
-    static constexpr size_t SMEM = ROWS * SMEM_PER_ROW;
+    static constexpr size_t SMEM = ROWS * SMEM_PER_ROW + (SB ? TeamFFTShared<real, N, E>::ENTRIES * sizeof(cplx<real>) : 0);
 
     const StageArgs<real>& a;
     int n, t;
@@ -692,9 +766,11 @@ struct RowKernel {
     real* keep;            // [NKEEP][N], point m at [slot][m]
     int inst;              // instance of this row
     size_t io;             // its buffer offset (complex elements)
-    TeamFFT<real, N, E> fft;
+    FFT fft;
 
-    __device__ cplx<real> yv(int q, int k) const { return a.Y[io + (size_t)q * N * H + (size_t)n * H + k]; }
+    // planes of the Y/G arrays hold ny rows of H
+    __device__ size_t plane() const { return (size_t)a.ny * H; }
+    __device__ cplx<real> yv(int q, int k) const { return a.Y[io + (size_t)q * plane() + (size_t)n * H + k]; }
 
     // half spectrum of physical field p at x wave number k in [1, H)
     __device__ cplx<real> xspec(int p, int k) const {
@@ -722,8 +798,8 @@ struct RowKernel {
 
     // C2R pair: v[e] = (field pa, field pb) at point m = t + TEAM e
     __device__ void c2r(int pa, int pb, cplx<real> (&v)[E]) {
-        const cplx<real> da = a.D[io + (size_t)pa * N + n];
-        const cplx<real> db = pb >= 0 ? a.D[io + (size_t)pb * N + n] : mk<real>(0, 0);
+        const cplx<real> da = a.D[io + (size_t)pa * a.ny + n];
+        const cplx<real> db = pb >= 0 ? a.D[io + (size_t)pb * a.ny + n] : mk<real>(0, 0);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int k = t + TEAM * e;
@@ -753,24 +829,24 @@ struct RowKernel {
         }
         if (t == 0) {
             const cplx<real> z0 = x.read(0), zh = x.read(H);
-            if (ep >= 0) a.Ed[io + (size_t)ep * N + n] = mk<real>(z0.x, zh.x);
-            if (eq >= 0) a.Ed[io + (size_t)eq * N + n] = mk<real>(z0.y, zh.y);
+            if (ep >= 0) a.Ed[io + (size_t)ep * a.ny + n] = mk<real>(z0.x, zh.x);
+            if (eq >= 0) a.Ed[io + (size_t)eq * a.ny + n] = mk<real>(z0.y, zh.y);
         }
         x.sync();
     }
 
-    __device__ cplx<real>* grow(int g) const { return a.G + io + (size_t)g * N * H + (size_t)n * H; }
+    __device__ cplx<real>* grow(int g) const { return a.G + io + (size_t)g * plane() + (size_t)n * H; }
     __device__ real& kp(int f, int e) const { return keep[f * N + t + TEAM * e]; }
     __device__ void zero_slot0(int g) const { if (t == 0) grow(g)[0] = mk<real>(0, 0); }
     __device__ void dump(int fld, const cplx<real> (&v)[E], bool imag) const {
         if (!a.phys_out) return;
-        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * N + (size_t)n * N;
+        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * a.ny + (size_t)n * N;
 #pragma unroll
         for (int e = 0; e < E; ++e) o[t + TEAM * e] = imag ? v[e].y : v[e].x;
     }
     __device__ void dump_slot(int fld, int slot) const {
         if (!a.phys_out) return;
-        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * N + (size_t)n * N;
+        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * a.ny + (size_t)n * N;
 #pragma unroll
         for (int e = 0; e < E; ++e) o[t + TEAM * e] = kp(slot, e);
     }
@@ -791,7 +867,7 @@ struct RowKernel {
     for (int e = 0; e < PH; ++e) { g0v[e] = mk<real>(0, 0); g1v[e] = g0v[e]; }
         // the column kernel that follows takes its work items from this counter
         if (a.queue && blockIdx.x == 0 && threadIdx.x == 0) *a.queue = 0;
-        fft.template init<N>(t, a.tw);
+        if constexpr (!SB) fft.template init<N>(t, a.tw);   // (MODE 1: filled by the kernel)
         for (int g = 0; g < NG; ++g) zero_slot0(g);
 
         // 1. r1, r2 -> slots 0, 1
@@ -914,17 +990,23 @@ struct RowKernel {
     }
 };
 
-template <typename real, int N, int E, int ROWS, int MINB>
+template <typename real, int N, int E, int ROWS, int MINB, int MODE = 0>
 __global__ void __launch_bounds__(ROWS * (N / E), MINB) row_kernel(const StageArgs<real> a) {
-    using K = RowKernel<real, N, E, ROWS>;
+    using K = RowKernel<real, N, E, ROWS, MODE>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int r = threadIdx.x / K::TEAM, t = threadIdx.x % K::TEAM;
     unsigned char* mine = smem_raw + (size_t)r * K::SMEM_PER_ROW;
-    constexpr int BLOCKS_PER_INST = N / ROWS;
+    const int BLOCKS_PER_INST = a.ny / ROWS;   // rows of an instance (ny) by ROWS per CTA
     const int inst = (int)blockIdx.x / BLOCKS_PER_INST;
     K k{a, ((int)blockIdx.x % BLOCKS_PER_INST) * ROWS + r, t,
         typename K::X{reinterpret_cast<cplx<real>*>(mine), 1 + r},
         reinterpret_cast<real*>(mine + N * sizeof(cplx<real>)), inst, (size_t)inst * a.istride, {}};
+    if constexpr (K::SB) {
+        cplx<real>* table = reinterpret_cast<cplx<real>*>(smem_raw + (size_t)ROWS * K::SMEM_PER_ROW);
+        if (r == 0) K::FFT::template fill<N>(table, t, a.tw);
+        k.fft.tab = table + t;
+        __syncthreads();
+    }
     static_assert(K::PH * K::TEAM == N / 2, "row team layout");
     k.run();
 }
@@ -934,23 +1016,25 @@ __global__ void __launch_bounds__(ROWS * (N / E), MINB) row_kernel(const StageAr
 // and the internal split layout (main[tidx(i, j)], nyq[j]).
 // ---------------------------------------------------------------------------
 template <typename real>
-__global__ void ref_to_internal(const cplx<real>* __restrict__ ref, cplx<real>* __restrict__ m, cplx<real>* __restrict__ nq, int N) {
-    const int H = N / 2, nxh = H + 1;
-    const size_t total = (size_t)nxh * N;
+__global__ void ref_to_internal(const cplx<real>* __restrict__ ref, cplx<real>* __restrict__ m, cplx<real>* __restrict__ nq, int nx,
+                                int ny) {
+    const int H = nx / 2, nxh = H + 1;
+    const size_t total = (size_t)nxh * ny;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
         const int j = (int)(k / nxh), i = (int)(k % nxh);
-        if (i < H) m[tidx(N, i, j)] = ref[k];
+        if (i < H) m[tidx(ny, i, j)] = ref[k];
         else nq[j] = ref[k];
     }
 }
 
 template <typename real>
-__global__ void internal_to_ref(const cplx<real>* __restrict__ m, const cplx<real>* __restrict__ nq, cplx<real>* __restrict__ ref, int N) {
-    const int H = N / 2, nxh = H + 1;
-    const size_t total = (size_t)nxh * N;
+__global__ void internal_to_ref(const cplx<real>* __restrict__ m, const cplx<real>* __restrict__ nq, cplx<real>* __restrict__ ref, int nx,
+                                int ny) {
+    const int H = nx / 2, nxh = H + 1;
+    const size_t total = (size_t)nxh * ny;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
         const int j = (int)(k / nxh), i = (int)(k % nxh);
-        ref[k] = (i < H) ? m[tidx(N, i, j)] : nq[j];
+        ref[k] = (i < H) ? m[tidx(ny, i, j)] : nq[j];
     }
 }
 

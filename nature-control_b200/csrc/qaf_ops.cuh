@@ -12,10 +12,12 @@
 
 namespace qaf {
 
+// N is the column length ny; the nx / 2 columns are the grid (tw: the ny-point twiddles)
 template <typename real, int N, int W, int E>
 __global__ void __launch_bounds__(W * (N / E))
-col_ifft_kernel(const cplx<real>* __restrict__ spec, cplx<real>* __restrict__ T, const cplx<real>* __restrict__ tw) {
-    constexpr int H = N / 2, TEAM = N / E, NXH = H + 1;
+col_ifft_kernel(const cplx<real>* __restrict__ spec, cplx<real>* __restrict__ T, const cplx<real>* __restrict__ tw, int nx) {
+    constexpr int TEAM = N / E;
+    const int H = nx / 2, NXH = H + 1;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<real>* buf = reinterpret_cast<cplx<real>*>(smem_raw);
     const int w = threadIdx.x % W, t = threadIdx.x / W;
@@ -23,7 +25,7 @@ col_ifft_kernel(const cplx<real>* __restrict__ spec, cplx<real>* __restrict__ T,
     XchgCols<real> x{buf, w, W};
     TeamFFT<real, N, E> fft;
     fft.template init<N>(t, tw);
-    const real s = (real)1 / ((real)N * (real)N);
+    const real s = (real)1 / ((real)nx * (real)N);
     cplx<real> v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -46,8 +48,9 @@ col_ifft_kernel(const cplx<real>* __restrict__ spec, cplx<real>* __restrict__ T,
 
 template <typename real, int N, int W, int E>
 __global__ void __launch_bounds__(W * (N / E))
-col_fft_kernel(const cplx<real>* __restrict__ T, cplx<real>* __restrict__ spec, const cplx<real>* __restrict__ tw) {
-    constexpr int H = N / 2, TEAM = N / E, NXH = H + 1;
+col_fft_kernel(const cplx<real>* __restrict__ T, cplx<real>* __restrict__ spec, const cplx<real>* __restrict__ tw, int nx) {
+    constexpr int TEAM = N / E;
+    const int H = nx / 2, NXH = H + 1;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<real>* buf = reinterpret_cast<cplx<real>*>(smem_raw);
     const int w = threadIdx.x % W, t = threadIdx.x / W;

@@ -23,14 +23,15 @@
 // that applies every multiplier in full and projects before transforming, so
 // the result equals the reference's also where the input is non-Hermitian.
 //
-// Internal layouts (N = nx = ny, H = N/2). The state is column-tiled so that
-// TW adjacent kx columns over all N rows form one contiguous slab (one TMA
+// Internal layouts (nx x ny grid, H = nx/2; the row kernel's transforms have
+// length nx, the column kernel's length ny). The state is column-tiled so that
+// TW adjacent kx columns over all ny rows form one contiguous slab (one TMA
 // bulk copy):
-//   spectral state, per field: main[tidx(i, j)] for kx index i < H, nyq[j] for i = H,
-//   tidx(i, j) = (i / TW) * N * TW + j * TW + i % TW
+//   spectral state, per field: main[tidx(ny, i, j)] for kx index i < H, nyq[j] for i = H,
+//   tidx(ny, i, j) = (i / TW) * ny * TW + j * TW + i % TW
 //   Y, G arrays: row-major [n * H + k] complex, k = x wave number (k = 0 slot
 //   unused); the column kernel fetches TW-column boxes of G with 2D TMA
-//   D (9 x N), Ed (10 x N): packed (DC + i*Nyquist) per row n
+//   D (9 x ny), Ed (10 x ny): packed (DC + i*Nyquist) per row n
 #pragma once
 
 #include "qaf_fft.cuh"
@@ -66,6 +67,7 @@ struct alignas(64) StageArgs {
     // 8-byte elements (two per FP64 complex), for the column kernel's TMA boxes
     CUtensorMap tm_G;
     // geometry and physics
+    int nx, ny;            // grid points along x (rows) and y (columns)
     real dkx, dky;         // 2 pi / Lx, 2 pi / Ly
     real lambda;           // flow alignment
     real ce;               // 1 / (Er Re)
@@ -84,16 +86,17 @@ struct alignas(64) StageArgs {
     cplx<real>* nl_m[3];
     cplx<real>* nl_n[3];
     // intermediates
-    cplx<real>* Y;         // NY * N * H
-    cplx<real>* D;         // PF_COUNT * N
-    cplx<real>* G;         // NG * N * H
-    cplx<real>* Ed;        // NE * N
+    cplx<real>* Y;         // NY planes of ny * nx/2
+    cplx<real>* D;         // PF_COUNT * ny
+    cplx<real>* G;         // NG planes of ny * nx/2
+    cplx<real>* Ed;        // NE * ny
     // tables
-    const cplx<real>* tw;  // tw[m] = exp(-2 pi i m / N), m < N
+    const cplx<real>* tw;    // tw[m] = exp(-2 pi i m / nx), m < nx (row transforms)
+    const cplx<real>* tw_y;  // tw_y[m] = exp(-2 pi i m / ny), m < ny (column transforms)
     // separable integrating factors: E(i,j) = ex[c][i] * ey[c][j] * e0[c]
     // c = 0: w full step, 1: w half step, 2: Q full step, 3: Q half step
-    const real* ex;        // 4 * (H + 1)
-    const real* ey;        // 4 * N
+    const real* ex;        // 4 * (nx / 2 + 1)
+    const real* ey;        // 4 * ny
     real e0[4];
     // stage control
     int mode, integrator, stage, last_stage, do_inverse;
@@ -104,7 +107,7 @@ struct alignas(64) StageArgs {
     int drop_slab;         // test hook, 0: off; k > 0: the column kernel arms slab k - 1 of
                            // queue item 0 (always a tile) without issuing its copy
     int* queue;            // work counter of the persistent column kernel (reset by the row kernel)
-    real* phys_out;        // optional: 9 physical fields + S + p11 p12 p21 (13 * N * N)
+    real* phys_out;        // optional: 9 physical fields + S + p11 p12 p21 (13 * nx * ny)
     int phys_all;          // with phys_out: also S, p11, p12, p21 (else the 9 fields only)
     size_t phys_istride;   // reals between instances' phys_out blocks
     // batches of independent instances of the same grid: every buffer above

@@ -56,8 +56,10 @@ namespace {
 
 struct Opts {
     std::string mode = "run";
-    int n = 128;
-    double L = 16.0 * M_PI;
+    int n = 128;               // nx (and ny unless --ny is given)
+    int ny = 0;                // 0: the same as n
+    double L = 16.0 * M_PI;    // Lx (and Ly unless --Ly is given)
+    double Ly = 0;
     double re = 1.0, er = 1.0, rf = 0.1, lambda = 0.1, alpha = 1.0, dt = 1e-3;
     int steps = 10;
     std::set<int> dumps;
@@ -82,7 +84,9 @@ Opts parse(int argc, char** argv) {
     for (int a = 2; a + 1 < argc; a += 2) {
         std::string k = argv[a]; const char* v = argv[a + 1];
         if (k == "--n") o.n = std::atoi(v);
+        else if (k == "--ny") o.ny = std::atoi(v);
         else if (k == "--L") o.L = std::atof(v);
+        else if (k == "--Ly") o.Ly = std::atof(v);
         else if (k == "--re") o.re = std::atof(v);
         else if (k == "--er") o.er = std::atof(v);
         else if (k == "--rf") o.rf = std::atof(v);
@@ -118,9 +122,10 @@ void analytic(const std::string& kind, double x, double y, double& w, double& r1
 }
 
 void make_init(const Opts& o, std::vector<double>& w, std::vector<double>& r1, std::vector<double>& r2) {
-    int n = o.n; size_t np = (size_t)n * n;
+    int n = o.n, ny = o.ny; size_t np = (size_t)n * ny;
     w.assign(np, 0); r1.assign(np, 0); r2.assign(np, 0);
-    if (o.init == "random") { qaf_random_q_init(o.seed, n, n, -0.01, 0.01, w.data(), r1.data(), r2.data()); return; }
+    if (o.init == "random") { qaf_random_q_init(o.seed, n, ny, -0.01, 0.01, w.data(), r1.data(), r2.data()); return; }
+    if (ny != n) die("--ny != --n: only --init random");
     if (o.init == "couple") { qaf_couple_init(o.seed, n, n, o.L, o.L, 1e-3, w.data(), r1.data(), r2.data()); return; }
     double dx = o.L / n;
     for (int j = 0; j < n; ++j) for (int i = 0; i < n; ++i) {
@@ -131,10 +136,11 @@ void make_init(const Opts& o, std::vector<double>& w, std::vector<double>& r1, s
 
 // Binary dump: "QAFDUMP1", int32 nx, ny, nxh, real_bytes, nfields, kind (0 spectral, 1 physical),
 // int64 step, then the fields back to back in the reference's layout.
-void dump(const std::string& path, int n, int kind, long long step, const std::vector<const void*>& dev, size_t bytes_each) {
+void dump(const std::string& path, int n, int ny, int kind, long long step, const std::vector<const void*>& dev,
+          size_t bytes_each) {
     FILE* f = std::fopen(path.c_str(), "wb");
     if (!f) die(("cannot write " + path).c_str());
-    int32_t hdr[6] = { n, n, n / 2 + 1, (int32_t)sizeof(Qreal), (int32_t)dev.size(), kind };
+    int32_t hdr[6] = { n, ny, n / 2 + 1, (int32_t)sizeof(Qreal), (int32_t)dev.size(), kind };
     std::fwrite("QAFDUMP1", 1, 8, f);
     std::fwrite(hdr, sizeof(hdr), 1, f);
     int64_t s = step; std::fwrite(&s, sizeof(s), 1, f);
@@ -157,7 +163,7 @@ struct Solver {
 
     Solver(const Opts& o) {
         const int BSZ_ = 16;
-        mesh = new Mesh(o.n, o.n, o.L, o.L, BSZ_);
+        mesh = new Mesh(o.n, o.ny, o.L, o.Ly, BSZ_);
         Nxh = mesh->Nxh; Ny = mesh->Ny; BSZ = BSZ_;
         re = o.re; er = o.er; rf = o.rf; lambda = o.lambda; dt = o.dt; do_dealias = o.dealias;
         wold = new Field(mesh); wcurr = new Field(mesh); wnew = new Field(mesh); wnonl = new Field(mesh);
@@ -171,7 +177,7 @@ struct Solver {
         std::vector<double> w0, r10, r20;
         make_init(o, w0, r10, r20);
         load(wold, w0); load(r1old, r10); load(r2old, r20);
-        std::vector<double> ra((size_t)o.n * o.n, o.alpha);
+        std::vector<double> ra((size_t)o.n * o.ny, o.alpha);
         std::vector<Qreal> rah(ra.begin(), ra.end());
         check(cudaMemcpy(Ra->phys, rah.data(), mesh->physsize, cudaMemcpyHostToDevice), "Ra");
 
@@ -251,10 +257,10 @@ std::string stepname(const std::string& out, int s) { return out + "_s" + std::t
 int run(const Opts& o) {
     Solver sv(o);
     size_t sb = sv.mesh->specsize;
-    if (o.dumps.count(0)) dump(stepname(o.out, 0), o.n, 0, 0, {sv.wold->spec, sv.r1old->spec, sv.r2old->spec}, sb);
+    if (o.dumps.count(0)) dump(stepname(o.out, 0), o.n, o.ny, 0, 0, {sv.wold->spec, sv.r1old->spec, sv.r2old->spec}, sb);
     for (int m = 1; m <= o.steps; ++m) {
         sv.step();
-        if (o.dumps.count(m)) dump(stepname(o.out, m), o.n, 0, m, {sv.wold->spec, sv.r1old->spec, sv.r2old->spec}, sb);
+        if (o.dumps.count(m)) dump(stepname(o.out, m), o.n, o.ny, 0, m, {sv.wold->spec, sv.r1old->spec, sv.r2old->spec}, sb);
     }
     check(cudaDeviceSynchronize(), "run");
     std::printf("{\"mode\": \"run\", \"n\": %d, \"steps\": %d, \"ok\": true}\n", o.n, o.steps);
@@ -267,8 +273,8 @@ int nonlinear(const Opts& o) {
     sv.nonlinear();
     check(cudaDeviceSynchronize(), "nonlinear");
     size_t sb = sv.mesh->specsize;
-    dump(o.out + "_nl.bin", o.n, 0, 0, {sv.wnonl->spec, sv.r1nonl->spec, sv.r2nonl->spec}, sb);
-    dump(o.out + "_in.bin", o.n, 0, 0, {sv.wold->spec, sv.r1old->spec, sv.r2old->spec}, sb);
+    dump(o.out + "_nl.bin", o.n, o.ny, 0, 0, {sv.wnonl->spec, sv.r1nonl->spec, sv.r2nonl->spec}, sb);
+    dump(o.out + "_in.bin", o.n, o.ny, 0, 0, {sv.wold->spec, sv.r1old->spec, sv.r2old->spec}, sb);
     std::printf("{\"mode\": \"nonlinear\", \"n\": %d, \"ok\": true}\n", o.n);
     return 0;
 }
@@ -368,7 +374,9 @@ int probe(const Opts& o) {
 
 int main(int argc, char** argv) {
     Opts o = parse(argc, argv);
-    if (o.n < 4 || (o.n % 2)) die("--n must be even and >= 4");
+    if (o.ny == 0) o.ny = o.n;
+    if (o.Ly == 0) o.Ly = o.L;
+    if (o.n < 4 || (o.n % 2) || o.ny < 4) die("--n must be even and >= 4, --ny >= 4");
     if (o.mode == "run") return run(o);
     if (o.mode == "nonlinear") return nonlinear(o);
     if (o.mode == "time") return timeit(o);

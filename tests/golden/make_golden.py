@@ -27,6 +27,11 @@ noted; seeded random Q ~ U(-0.01, 0.01), w = 0, generator include/qaf_init.h):
                          evaluation at 96^2 and 192^2 (seeds 12 / 13) and
                          IF-RK4 dt = 1e-3 at 96^2 and 192^2 (seeds 14 / 15),
                          states at steps 0 1 20
+  rect                   grids with nx != ny (Mesh(Nx, Ny, Lx, Ly), Mesh.cuh:61-73):
+                         one nonlinear evaluation at 96 x 64 (Lx = 16 pi,
+                         Ly = 32 pi / 3, the same spacing; seed 16) and IF-RK4
+                         dt = 1e-3 at 64 x 128 (Lx = 16 pi, Ly = 32 pi; seed 17),
+                         states at steps 0 1 20
   kat summary            the reference's nonlinear terms for the analytic input
                          sets of UnitTest/Nonlinear/nlterms0-4 (N = 128, L = 2 pi,
                          Re = Er = 0.1, Ra = 0.2), reduced to their deviation from
@@ -51,7 +56,10 @@ import oracle as O  # noqa: E402
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 TWO_PI = "6.283185307179586"
 EIGHT_PI = "25.132741228718345"
-GROUPS = ("nl", "run32", "run64", "run128", "kat", "couple64", "dealiasw64", "grid3")
+GROUPS = ("nl", "run32", "run64", "run128", "kat", "couple64", "dealiasw64", "grid3", "rect")
+SIXTEEN_PI = "50.26548245743669"
+THIRTYTWO_PI = "100.53096491487338"
+THIRTYTWO_PI_3 = "33.510321638291124"
 GRID3_STEPS = (0, 1, 20)
 COUPLE_STEPS = (0, 1, 10, 1000)
 DEALIASW_STEPS = (0, 1, 10, 200)
@@ -84,6 +92,10 @@ def run_harness(out, only=GROUPS):
                    ",".join(str(s) for s in GRID3_STEPS), "--out", f"{out}/run96"],
                   [H, "run", "--n", "192", "--steps", "20", "--seed", "15", "--dumps",
                    ",".join(str(s) for s in GRID3_STEPS), "--out", f"{out}/run192"]],
+        "rect": [[H, "nonlinear", "--n", "96", "--ny", "64", "--L", SIXTEEN_PI, "--Ly", THIRTYTWO_PI_3, "--init",
+                  "random", "--seed", "16", "--out", f"{out}/nl_rect96x64"],
+                 [H, "run", "--n", "64", "--ny", "128", "--L", SIXTEEN_PI, "--Ly", THIRTYTWO_PI, "--steps", "20",
+                  "--seed", "17", "--dumps", ",".join(str(s) for s in GRID3_STEPS), "--out", f"{out}/run64x128"]],
     }
     for name in only:
         for c in jobs[name]:
@@ -149,6 +161,10 @@ def convert(d, only=GROUPS):
         save("ref_couple64.npz", **states("couple64", COUPLE_STEPS))
     if "dealiasw64" in only:
         save("ref_dealiasw64.npz", **states("dealiasw64", DEALIASW_STEPS))
+    if "rect" in only:
+        i, nl = f("nl_rect96x64_in.bin"), f("nl_rect96x64_nl.bin")
+        save("ref_nl_rect96x64.npz", w=i[0], r1=i[1], r2=i[2], wn=nl[0], r1n=nl[1], r2n=nl[2])
+        save("ref_run64x128.npz", **states("run64x128", GRID3_STEPS))
     if "grid3" in only:
         for n in (96, 192):
             i, nl = f(f"nl_rand{n}_in.bin"), f(f"nl_rand{n}_nl.bin")

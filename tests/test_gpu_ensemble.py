@@ -51,8 +51,13 @@ def test_mixed_sizes_match_single_meshes(cuda, dtype, tol):
         ew, er1, er2 = ens.store(k)
         for got, want in ((ew, w), (er1, r1), (er2, r2)):
             assert _rel(got, want) <= tol, (k, n)
+        # energy and enstrophy are quadratic in the state: about twice its
+        # relative difference (the batch and single-grid column kernels may
+        # differ in their shared/register twiddles and inlining, i.e. in FP32
+        # rounding)
         e2, z2 = diags[k]
-        assert abs(e2 - e1) <= 1e-9 * abs(e1) and abs(z2 - z1) <= 1e-9 * abs(z1), (k, e1, e2, z1, z2)
+        dtol = 1e-9 if dtype == "F64" else 4 * tol
+        assert abs(e2 - e1) <= dtol * abs(e1) and abs(z2 - z1) <= dtol * abs(z1), (k, e1, e2, z1, z2)
 
 
 def test_many_instances_fp32(cuda):

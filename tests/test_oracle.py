@@ -154,6 +154,28 @@ def test_rk4_steps_match_reference_build_3x2k(n):
             assert O.rel_l2(a, g[f"{name}_{s}"]) < 1e-14, (s, name)
 
 
+def test_rect_grids_match_reference_build():
+    # nx != ny, Lx != Ly: one nonlinear evaluation at 96 x 64 and 20 IF-RK4
+    # steps at 64 x 128, each against the reference's build (Mesh(Nx, Ny, Lx, Ly))
+    g = golden("ref_nl_rect96x64.npz")
+    p = O.params(n=96, ny=64, L=16 * np.pi, Ly=16 * np.pi * 64 / 96)
+    out = O.nonlinear(p, g["w"], g["r1"], g["r2"])
+    for a, b in zip(out, (g["wn"], g["r1n"], g["r2n"])):
+        assert O.rel_l2(a, b) < 5e-15
+    g = golden("ref_run64x128.npz")
+    p = O.params(n=64, ny=128, L=16 * np.pi, Ly=32 * np.pi)
+    w, r1, r2 = O.initial_spectra(17, 64, ny=128)
+    for a, name in zip((w, r1, r2), ("w_0", "r1_0", "r2_0")):
+        assert O.rel_l2(O.hermitian_part(a), O.hermitian_part(g[name])) < 1e-15
+    st = (g["w_0"], g["r1_0"], g["r2_0"])
+    prev = 0
+    for s in (1, 20):
+        st = O.step(p, *st, s - prev)
+        prev = s
+        for a, name in zip(st, ("w", "r1", "r2")):
+            assert O.rel_l2(a, g[f"{name}_{s}"]) < 1e-14, (s, name)
+
+
 def test_rk4_100_steps_match_reference_build_64():
     g = golden("ref_run64_s100.npz")
     p = O.params(n=64)
