@@ -676,11 +676,11 @@ __global__ void __launch_bounds__(NGA * (N / 2 / E)) adj_row_kernel(const __grid
 }
 
 // loss += weight * (0.5 / N^4) * diag[0] (the enstrophy sum of the step's new state); weight carries 1/N^4
-__global__ void adj_loss_accumulate(const double* diag, double* loss, double weight) {
+static __global__ void adj_loss_accumulate(const double* diag, double* loss, double weight) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *loss += weight * 0.5 * diag[0];
 }
 // the same for ninst instances (diag: 2 doubles per instance)
-__global__ void adj_loss_accumulate_batch(const double* diag, double* loss, double weight, int ninst) {
+static __global__ void adj_loss_accumulate_batch(const double* diag, double* loss, double weight, int ninst) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < ninst) loss[k] += weight * 0.5 * diag[2 * k];
 }

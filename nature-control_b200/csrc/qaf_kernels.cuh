@@ -98,7 +98,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsign
 // N is the column length ny (the y-transforms' length); the number of
 // kx-columns H = nx / 2, and with it the tiles and work items, is a launch
 // argument.
-template <typename real, int N, int E, int MODE = 0>
+template <typename real, int N, int E, int MODE = 0, bool SQ = true>
 struct ColKernel {
     static constexpr int TEAM = N / E, NTHREADS = TW * TEAM;
     static constexpr size_t SLAB = (size_t)N * TW;   // complex elements of one slab
@@ -141,7 +141,6 @@ struct ColKernel {
     const StageArgs<real>& a;
     const FFT& fft;
     int t, w;
-    int H;                 // kx-columns nx / 2 (the last, kx = H, is an edge column)
     cplx<real>* bufs;      // three slab buffers back to back
     uint64_t* mbar;        // one mbarrier per buffer
     volatile int* aborted; // shared: a wait of this CTA ran out
@@ -160,6 +159,14 @@ struct ColKernel {
     unsigned withheld;     // thread 0: the buffer of the test hook's withheld copy (NBUF: none)
 
     __device__ cplx<real>* buf(int b) const { return bufs + (size_t)b * SLAB; }
+    // kx-columns nx / 2 (the last, kx = nx/2, is an edge column): N / 2 at
+    // compile time on a square grid (SQ), which keeps the index arithmetic in
+    // shifts and immediates (with the size at run time the 1024^2 kernels
+    // spilled), else from the launch arguments
+    __device__ __forceinline__ int Hx() const {
+        if constexpr (SQ) return N / 2;
+        else return a.nx / 2;
+    }
     __device__ int nG(int f) const { return a.mode == MODE_PROLOGUE ? 0 : (f == 0 ? 3 : 2); }
     __device__ int per_field(int f) const { return nG(f) + (need_old ? 1 : 0) + (need_acc ? 1 : 0); }
     // slab sidx of the item: a G array (>= 0: its plane index) or a state slab (pointer)
@@ -201,7 +208,7 @@ struct ColKernel {
 #pragma unroll 1
                     for (int r0 = 0; r0 < N; r0 += BOXR)
                         tile_load_2d(buf(b) + (size_t)r0 * TW, &a.tm_G, T * TW * CPE,
-                                     (int)((io / (size_t)H) + (size_t)g * N + r0), &mbar[b]);
+                                     (int)((io / (size_t)Hx()) + (size_t)g * N + r0), &mbar[b]);
                 } else {
                     bulk_load(buf(b), slab_state(next), bytes, &mbar[b]);
                 }
@@ -257,7 +264,7 @@ struct ColKernel {
         const int i = T * TW + w;
         const bool edge_col = (i == 0);   // kx = 0 belongs to the edge item
         const real kx = a.dkx * (real)i;
-        const real sc = (real)1 / ((real)a.nx * (real)a.ny);
+        const real sc = SQ ? (real)1 / ((real)N * (real)N) : (real)1 / ((real)a.nx * (real)a.ny);
         const int ng = nG(f);
         const size_t base = io + (size_t)T * SLAB;
         cplx<real> nl[E], curr[E];
@@ -286,8 +293,8 @@ struct ColKernel {
         } else {
             const int cls = f == 0 ? 0 : 2;
             const real* e0 = a.inst_e0 ? a.inst_e0 + 4 * inst : a.e0;
-            const real exf = table(&a.ex[cls * (H + 1) + i]) * e0[cls];
-            const real exh = table(&a.ex[(cls + 1) * (H + 1) + i]) * e0[cls + 1];
+            const real exf = table(&a.ex[cls * (Hx() + 1) + i]) * e0[cls];
+            const real exh = table(&a.ex[(cls + 1) * (Hx() + 1) + i]) * e0[cls + 1];
             // the y factors of PF elements at a time first (through the
             // read-only path when PF > 1): fetched inside the loop, each load
             // would wait behind the previous element's stores (the compiler
@@ -388,9 +395,9 @@ struct ColKernel {
             }
             if constexpr (DB) fft.template run_db<true, SWZ>(t, v, xbuf, buf(sx % NBUF), w, TW);
             else fft.template run<true>(t, v, x);
-            cplx<real>* Y = a.Y + io + (size_t)q * N * H + i;
+            cplx<real>* Y = a.Y + io + (size_t)q * N * Hx() + i;
 #pragma unroll
-            for (int e = 0; e < E; ++e) Y[(size_t)(t + TEAM * e) * H] = v[e];
+            for (int e = 0; e < E; ++e) Y[(size_t)(t + TEAM * e) * Hx()] = v[e];
             if constexpr (!DB) x.sync();   // the next transform reuses the buffer
         }
         issue_upto(sx + NBUF + 1);
@@ -446,17 +453,17 @@ __device__ __forceinline__ void edge_product_mults(int p, real ky, real kN, real
     }
 }
 
-template <typename real, int N, int W, int E>
+template <typename real, int N, int W, int E, bool SQ = true>
 __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int inst, int t, int w, cplx<real>* buf,
                                          cplx<real>* ctab) {
     const size_t io = (size_t)inst * a.istride;
     constexpr int TEAM = N / E;
-    const int H = a.nx / 2;   // the kx = nx/2 column
+    const int H = SQ ? N / 2 : a.nx / 2;   // the kx = nx/2 column
     XchgCols<real> x{buf, w, W};
     TeamFFT<real, N, E> fft;
     fft.template init<N>(t, a.tw_y);
     const real kN = a.dkx * (real)H;
-    const real s = (real)1 / ((real)a.nx * (real)a.ny);
+    const real s = SQ ? (real)1 / ((real)N * (real)N) : (real)1 / ((real)a.nx * (real)a.ny);
     cplx<real> v[E];
     // N^ of columns kx = 0 (ctab[j]) and kx = N/2 (ctab[N + j]), summed over
     // the products in shared memory; team 0 owns every j of a column
@@ -643,9 +650,9 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int in
     }
 }
 
-template <typename real, int N, int E, int MINB, int MODE = 0>
+template <typename real, int N, int E, int MINB, int MODE = 0, bool SQ = true>
 __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_constant__ StageArgs<real> a) {
-    using K = ColKernel<real, N, E, MODE>;
+    using K = ColKernel<real, N, E, MODE, SQ>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cplx<real>* bufs = reinterpret_cast<cplx<real>*>(smem_raw);
     const int tid = threadIdx.x, w = tid % TW, t = tid / TW;
@@ -682,7 +689,7 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();   // barriers initialised, twiddle table filled
-    K k{a, fft, t, w, a.nx / 2, bufs, mbar, aborted, 0u, 0, 0, 0, 0, 0, 0, false, false};
+    K k{a, fft, t, w, bufs, mbar, aborted, 0u, 0, 0, 0, 0, 0, 0, false, false};
     k.red = red;
     k.xbuf = xbuf;
     k.eys = eys;
@@ -690,7 +697,7 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
     k.withheld = (unsigned)K::NBUF;
     // item q of the launch: kind-major over instances (all r1+r2 tiles of all
     // instances first, then the w tiles, then the edge columns)
-    const int tiles = k.H / TW;
+    const int tiles = k.Hx() / TW;
     const int total = (2 * tiles + 3) * a.ninst;
     for (;;) {
         if (tid == 0) *item_sh = atomicAdd(a.queue, 1);
@@ -712,7 +719,7 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
             if constexpr (K::INLINE_ITEM) k.item_body(0, -1, local - tiles, inst);
             else k.item(0, -1, local - tiles, inst);
         } else {
-            col_edge<real, N, TW, E>(a, local - 2 * tiles, inst, t, w, bufs, ctab);
+            col_edge<real, N, TW, E, SQ>(a, local - 2 * tiles, inst, t, w, bufs, ctab);
             __syncthreads();
         }
     }
@@ -748,7 +755,7 @@ struct XchgTeam {
 
 // MODE 1: the twiddle bases in a shared table after the rows' regions
 // (TeamFFTShared), shared by the CTA's row teams
-template <typename real, int N, int E, int ROWS, int MODE = 0>
+template <typename real, int N, int E, int ROWS, int MODE = 0, bool SQ = true>
 struct RowKernel {
     static constexpr int H = N / 2, TEAM = N / E, PH = E / 2;
     static constexpr bool SB = MODE >= 1;
@@ -769,7 +776,12 @@ struct RowKernel {
     FFT fft;
 
     // planes of the Y/G arrays hold ny rows of H
-    __device__ size_t plane() const { return (size_t)a.ny * H; }
+    // rows ny: N at compile time on a square grid (SQ), else from the launch arguments
+    __device__ __forceinline__ int ny() const {
+        if constexpr (SQ) return N;
+        else return a.ny;
+    }
+    __device__ size_t plane() const { return (size_t)ny() * H; }
     __device__ cplx<real> yv(int q, int k) const { return a.Y[io + (size_t)q * plane() + (size_t)n * H + k]; }
 
     // half spectrum of physical field p at x wave number k in [1, H)
@@ -798,8 +810,8 @@ struct RowKernel {
 
     // C2R pair: v[e] = (field pa, field pb) at point m = t + TEAM e
     __device__ void c2r(int pa, int pb, cplx<real> (&v)[E]) {
-        const cplx<real> da = a.D[io + (size_t)pa * a.ny + n];
-        const cplx<real> db = pb >= 0 ? a.D[io + (size_t)pb * a.ny + n] : mk<real>(0, 0);
+        const cplx<real> da = a.D[io + (size_t)pa * ny() + n];
+        const cplx<real> db = pb >= 0 ? a.D[io + (size_t)pb * ny() + n] : mk<real>(0, 0);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int k = t + TEAM * e;
@@ -829,8 +841,8 @@ struct RowKernel {
         }
         if (t == 0) {
             const cplx<real> z0 = x.read(0), zh = x.read(H);
-            if (ep >= 0) a.Ed[io + (size_t)ep * a.ny + n] = mk<real>(z0.x, zh.x);
-            if (eq >= 0) a.Ed[io + (size_t)eq * a.ny + n] = mk<real>(z0.y, zh.y);
+            if (ep >= 0) a.Ed[io + (size_t)ep * ny() + n] = mk<real>(z0.x, zh.x);
+            if (eq >= 0) a.Ed[io + (size_t)eq * ny() + n] = mk<real>(z0.y, zh.y);
         }
         x.sync();
     }
@@ -840,13 +852,13 @@ struct RowKernel {
     __device__ void zero_slot0(int g) const { if (t == 0) grow(g)[0] = mk<real>(0, 0); }
     __device__ void dump(int fld, const cplx<real> (&v)[E], bool imag) const {
         if (!a.phys_out) return;
-        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * a.ny + (size_t)n * N;
+        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * ny() + (size_t)n * N;
 #pragma unroll
         for (int e = 0; e < E; ++e) o[t + TEAM * e] = imag ? v[e].y : v[e].x;
     }
     __device__ void dump_slot(int fld, int slot) const {
         if (!a.phys_out) return;
-        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * a.ny + (size_t)n * N;
+        real* o = a.phys_out + a.phys_istride * inst + (size_t)fld * N * ny() + (size_t)n * N;
 #pragma unroll
         for (int e = 0; e < E; ++e) o[t + TEAM * e] = kp(slot, e);
     }
@@ -990,13 +1002,13 @@ struct RowKernel {
     }
 };
 
-template <typename real, int N, int E, int ROWS, int MINB, int MODE = 0>
+template <typename real, int N, int E, int ROWS, int MINB, int MODE = 0, bool SQ = true>
 __global__ void __launch_bounds__(ROWS * (N / E), MINB) row_kernel(const StageArgs<real> a) {
-    using K = RowKernel<real, N, E, ROWS, MODE>;
+    using K = RowKernel<real, N, E, ROWS, MODE, SQ>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int r = threadIdx.x / K::TEAM, t = threadIdx.x % K::TEAM;
     unsigned char* mine = smem_raw + (size_t)r * K::SMEM_PER_ROW;
-    const int BLOCKS_PER_INST = a.ny / ROWS;   // rows of an instance (ny) by ROWS per CTA
+    const int BLOCKS_PER_INST = (SQ ? N : a.ny) / ROWS;   // rows of an instance (ny) by ROWS per CTA
     const int inst = (int)blockIdx.x / BLOCKS_PER_INST;
     K k{a, ((int)blockIdx.x % BLOCKS_PER_INST) * ROWS + r, t,
         typename K::X{reinterpret_cast<cplx<real>*>(mine), 1 + r},

@@ -290,7 +290,7 @@ __global__ void diag_kernel(Geo g, const cplx<real>* w, double* acc, const doubl
 }
 
 // energy, enstrophy of the last step from its sums (Parseval form), for an asynchronous read-back
-__global__ void diag_finalize_kernel(const double* sums, double* out, double n4) {
+static __global__ void diag_finalize_kernel(const double* sums, double* out, double n4) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         out[0] = 0.5 * sums[1] / n4;
         out[1] = 0.5 * sums[0] / n4;

@@ -71,7 +71,9 @@ StepVariant<float> v256[] = {make<ColV<256, 16>>("col:e16", 0), make<ColV<256, 8
                              make<RowV<256, 16, 8>>("row:e16r8", 1), make<RowV<256, 8, 8, 3>>("row:e8r8m3", 1)};
 StepVariant<float> v1024[] = {make<ColV<1024, 16>>("col:e16", 0), make<ColV<1024, 8, 2, 1>>("col:e8s", 0),
                               make<ColV<1024, 8>>("col:e8", 0), make<RowV<1024, 8, 1>>("row:e8r1", 1),
-                              make<RowV<1024, 16, 4>>("row:e16r4", 1), make<RowV<1024, 8, 1, 7>>("row:e8r1m7", 1)};
+                              make<RowV<1024, 16, 4>>("row:e16r4", 1), make<RowV<1024, 8, 1, 7>>("row:e8r1m7", 1),
+                              make<RowV<1024, 4, 4, 1>>("row:e4r4", 1), make<RowV<1024, 4, 4, 1, 1>>("row:e4r4s", 1),
+                              make<RowV<1024, 4, 2, 2, 1>>("row:e4r2s", 1)};
 
 }  // namespace
 
