@@ -145,8 +145,12 @@ qaf_status qaf_step_host(qaf_mesh* mesh, const qaf_params* p, qaf_integrator int
 qaf_status qaf_last_diagnostics(qaf_mesh* mesh, double out[2]);
 /* The same two values without synchronising: enqueued on `stream` (after the
  * steps it follows), written to `out` (2 doubles, pinned host or device
- * memory) when the stream reaches it. No counterpart in the reference. The
- * non-finite status is left to qaf_last_diagnostics / qaf_check_finite. */
+ * memory) when the stream reaches it. Where the device can address `out`
+ * (device memory, or page-locked host memory mapped under unified
+ * addressing) a kernel stores the values there directly, with no copy in
+ * the stream; other memory gets a staged copy. No counterpart in the
+ * reference. The non-finite status is left to qaf_last_diagnostics /
+ * qaf_check_finite. */
 qaf_status qaf_last_diagnostics_async(qaf_mesh* mesh, double* out, void* stream);
 /* Synchronises `stream` and reports whether any step since the last call
  * produced a non-finite value (the reference's NaN check, friction.cu:280). */

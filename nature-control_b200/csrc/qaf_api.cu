@@ -1003,6 +1003,25 @@ qaf_status qaf_last_diagnostics_async(qaf_mesh* m, double* out, void* stream) {
     if (!diag) return fail(QAF_ERR_INVALID, "no step has run on this mesh");
     cudaStream_t st = (cudaStream_t)stream;
     const double n4 = (double)m->desc.nx * m->desc.ny * (double)m->desc.nx * m->desc.ny;
+    // The kernel stores the two values where the device can address `out`
+    // directly: device memory of the current device, or page-locked host
+    // memory mapped into the device's address space (the same pointer under
+    // unified addressing). A copy operation in the stream would hold the
+    // stream's next kernel back for a PCIe round trip (~20-30 us per step);
+    // plain stores from the kernel are posted and visible to the host once
+    // the stream has been synchronised. Other memory takes the staged copy.
+    double* direct = nullptr;
+    int dev = 0;
+    cudaPointerAttributes pa;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaPointerGetAttributes(&pa, out) == cudaSuccess) {
+        if (pa.type == cudaMemoryTypeDevice && pa.device == dev) direct = out;
+        else if (pa.type == cudaMemoryTypeHost && pa.devicePointer) direct = static_cast<double*>(pa.devicePointer);
+    }
+    cudaGetLastError();   // an unregistered host pointer leaves an error behind
+    if (direct) {
+        diag_finalize_kernel<<<1, 32, 0, st>>>(diag, direct, n4);
+        return post_launch("qaf_last_diagnostics_async");
+    }
     double* staged = diag + 4 + 512 + 513;
     diag_finalize_kernel<<<1, 32, 0, st>>>(diag, staged, n4);
     QAF_TRY(post_launch("qaf_last_diagnostics_async"));
