@@ -236,16 +236,18 @@ __device__ __forceinline__ cplx<real> derived(int p, cplx<real> c, real kx, real
 }
 
 // The Y arrays a field feeds and their multipliers (main columns)
+// (1/k^2 is formed only for the three multipliers that use it)
 template <typename real>
 __device__ __forceinline__ cplx<real> y_mult(int q, cplx<real> c, real ky, real k2, real s) {
-    const real ik2 = k2 > (real)0 ? (real)1 / k2 : (real)0;
     switch (q) {
         case 0: case 1: case 2: return cscale(c, s);
-        case 3: return cmul_i(cscale(c, ky * ik2 * s));     // u^ = i ky w / k^2
-        case 4: return cscale(c, -ik2 * s);                 // psi^ = -w / k^2
-        case 5: return cscale(c, -ky * ky * ik2 * s);       // ky^2 psi^
-        default: return cscale(c, ky * ky * s);             // ky^2 r
+        case 6: case 7: return cscale(c, ky * ky * s);      // ky^2 r
+        default: break;
     }
+    const real ik2 = k2 > (real)0 ? (real)1 / k2 : (real)0;
+    if (q == 3) return cmul_i(cscale(c, ky * ik2 * s));     // u^ = i ky w / k^2
+    if (q == 4) return cscale(c, -ik2 * s);                 // psi^ = -w / k^2
+    return cscale(c, -ky * ky * ik2 * s);                   // ky^2 psi^ (q = 5)
 }
 
 }  // namespace qaf
