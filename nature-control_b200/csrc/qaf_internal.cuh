@@ -124,11 +124,21 @@ struct Cfg {
     // from 512^2 and every batch (ensemble) launch; otherwise register
     // twiddle bases (mode 0: for single small grids, whose launches are
     // latency-bound, the table's fill at kernel start measured slower)
+    //
+    // The small FP32 grids take the shapes that timed fastest on the B200
+    // when every shape was timed on one box (single grid and an 85-instance
+    // batch each): 64^2 four values per column thread (26-28% faster than
+    // eight), 256^2 batches six column CTAs per SM with register twiddle
+    // bases (2%), 128^2 and 256^2 single grids two rows per row CTA (5-9%).
     static constexpr bool WIDE1024 = F32 && N == 1024;
-    static constexpr int ECS = WIDE1024 ? 4 : EC;
+    static constexpr int ECS = WIDE1024 || (F32 && N == 64) ? 4 : EC;
     static constexpr int COL_MODE = WIDE1024 ? QAF_COL1024_MODE : (((F32 && N == 768) || (!F32 && N >= 512)) ? 1 : 0);
-    static constexpr int COL_MODE_B = WIDE1024 ? QAF_COL1024_MODE : 1;   // batches of instances
+    // batches of instances
+    static constexpr int COL_MODE_B = WIDE1024 ? QAF_COL1024_MODE : ((F32 && (N == 64 || N == 256)) ? 0 : 1);
     static constexpr int MINBC = WIDE1024 ? 1 : MINB;
+    static constexpr int MINBC_B = (F32 && N == 256) ? 6 : MINBC;
+    // batches launch their own kernel where its shape differs from the single grids'
+    static constexpr bool SEP_B = COL_MODE_B != COL_MODE || MINBC_B != MINBC;
     static constexpr int COL_THREADS = TW * (N / ECS);
     static constexpr size_t COL_SMEM = ColKernel<real, N, ECS, COL_MODE>::SMEM;
     static constexpr size_t COL_SMEM_B = ColKernel<real, N, ECS, COL_MODE_B>::SMEM;
@@ -143,6 +153,11 @@ struct Cfg {
     static constexpr int ROW_THREADS = ROWS * TEAM_R;
     static constexpr size_t ROW_SMEM = RowKernel<real, N, ER, ROWS>::SMEM;
     static_assert(16 % ROWS == 0, "rows per CTA divide every row count");
+    // square single grids (ninst == 1): two rows per CTA at 128^2 and 256^2 FP32
+    static constexpr int ROWS_S = (F32 && (N == 128 || N == 256)) ? 2 : ROWS;
+    static constexpr int ROW_THREADS_S = ROWS_S * TEAM_R;
+    static constexpr size_t ROW_SMEM_S = RowKernel<real, N, ER, ROWS_S>::SMEM;
+    static_assert(16 % ROWS_S == 0, "rows per CTA divide every row count");
     // standalone transforms: W kx-columns per CTA, half-length row FFTs
     static constexpr int W = 4 < H ? 4 : H;
     static constexpr int COLT_THREADS = W * (N / EC);

@@ -17,12 +17,12 @@ DeviceOnce Launch<real, N>::col_slots_b;
 template <typename real, int N>
 qaf_status Launch<real, N>::setup() {
     QAF_TRY(col_slots_b.get(nullptr, [](int* slots) -> qaf_status {
-        QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE_B>,
+        QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::ECS, C::MINBC_B, C::COL_MODE_B>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM_B));
         int dev = 0, sms = 0, per_sm = 0;
         QAF_CUDA(cudaGetDevice(&dev));
         QAF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        QAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE_B>,
+        QAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_kernel<real, N, C::ECS, C::MINBC_B, C::COL_MODE_B>,
                                                                C::COL_THREADS, C::COL_SMEM_B));
         if (per_sm < 1) return fail(QAF_ERR_UNSUPPORTED, "column kernel does not fit on an SM");
         *slots = sms * per_sm;
@@ -31,6 +31,8 @@ qaf_status Launch<real, N>::setup() {
     return col_slots.get(nullptr, [](int* slots) -> qaf_status {
         QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
         QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::ROW_SMEM));
+        QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS_S, C::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)C::ROW_SMEM_S));
         // the same kernels for grids with nx != ny (sizes from the launch arguments)
         QAF_CUDA(cudaFuncSetAttribute(col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COL_SMEM));
@@ -72,10 +74,10 @@ void Launch<real, N>::col(const StageArgs<real>& a0, cudaStream_t st) {
         }
     }
     const long items = (long)(2 * (a.nx / 2 / TW) + 3) * a.ninst;
-    if (a.ninst > 1 && C::COL_MODE_B != C::COL_MODE) {
+    if (a.ninst > 1 && C::SEP_B) {
         const int slots = col_slots_b.peek();
         const int grid = slots > 0 && items > slots ? slots : (int)items;
-        col_kernel<real, N, C::ECS, C::MINBC, C::COL_MODE_B><<<grid, C::COL_THREADS, C::COL_SMEM_B, st>>>(a);
+        col_kernel<real, N, C::ECS, C::MINBC_B, C::COL_MODE_B><<<grid, C::COL_THREADS, C::COL_SMEM_B, st>>>(a);
         return;
     }
     const int slots = col_slots.peek();   // set up by every operation before its launches
@@ -97,7 +99,9 @@ void Launch<real, N>::row(const StageArgs<real>& a, cudaStream_t st) {
             }
         }
     }
-    if (a.ny == N)
+    if (a.ny == N && a.ninst == 1)
+        row_kernel<real, N, C::ER, C::ROWS_S, C::MINB><<<a.ny / C::ROWS_S, C::ROW_THREADS_S, C::ROW_SMEM_S, st>>>(a);
+    else if (a.ny == N)
         row_kernel<real, N, C::ER, C::ROWS, C::MINB><<<(a.ny / C::ROWS) * a.ninst, C::ROW_THREADS, C::ROW_SMEM, st>>>(a);
     else
         row_kernel<real, N, C::ER, C::ROWS, C::MINB, 0, false>

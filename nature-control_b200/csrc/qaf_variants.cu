@@ -1,6 +1,7 @@
 // qaf_variants.cu — FP32 launch variants of the fused step kernels for the
-// autotuner (see qaf_variants.cuh): column kernel with 16 (or, at 64^2, 4)
-// values per thread of the y-FFT instead of 8, or a tighter register budget
+// autotuner (see qaf_variants.cuh): column kernel with 16 (or, at 64^2, 4 —
+// the built-in shape there since it timed fastest) values per thread of the
+// y-FFT instead of 8, or a tighter register budget
 // (more resident CTAs); at 1024^2, where the built-in column kernel takes 4
 // values per thread in one 1024-thread CTA per SM, the 8-value two-CTA
 // shapes (twiddle bases in shared memory or in registers); row kernel with
