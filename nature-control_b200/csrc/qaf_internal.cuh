@@ -139,6 +139,13 @@ struct Cfg {
     static constexpr int MINBC_B = (F32 && N == 256) ? 6 : MINBC;
     // batches launch their own kernel where its shape differs from the single grids'
     static constexpr bool SEP_B = COL_MODE_B != COL_MODE || MINBC_B != MINBC;
+    // single square grids of 32^2, 128^2 and 256^2: the field-parallel column
+    // pass (colfp_kernel, one CTA per kx-column running all of its transforms
+    // at once). Measured per step on one box, in CUDA graphs: 32^2 116 us
+    // against 136 us, 128^2 127 against 150 (the persistent kernel's best
+    // shape), 256^2 140 against 155; at 64^2 the persistent kernel stays
+    // faster (102-106 against 126)
+    static constexpr bool COL_FP = N == 32 || N == 128 || N == 256;
     static constexpr int COL_THREADS = TW * (N / ECS);
     static constexpr size_t COL_SMEM = ColKernel<real, N, ECS, COL_MODE>::SMEM;
     static constexpr size_t COL_SMEM_B = ColKernel<real, N, ECS, COL_MODE_B>::SMEM;

@@ -650,6 +650,153 @@ __device__ __forceinline__ void col_edge(const StageArgs<real>& a, int f, int in
     }
 }
 
+// ---------------------------------------------------------------------------
+// Field-parallel column pass of one small square grid (32^2, 128^2 or
+// 256^2, a single instance). The persistent kernel's CTA runs an item's seven or eight
+// y-transforms one after another, and a small grid has too few items to fill
+// the GPU with them; here one CTA per kx-column runs all of that column's
+// transforms at once — NTF = 8 teams, one per G array in the forward phase
+// (the eighth idle), one per Y array in the inverse phase — so a CTA's chain
+// is one forward transform, the stage update of the three fields and one
+// inverse transform. The last three CTAs take the kx = 0 / N/2 edge columns
+// of w, r1 and r2 (col_edge, the persistent kernel's edge item).
+// The arithmetic of every value is the persistent kernel's (the same
+// transforms, products and stage formulas in the same order); only the
+// diagnostics' partial sums are added in another order.
+// ---------------------------------------------------------------------------
+template <typename real, int N, int E>
+struct ColFP {
+    static constexpr int TEAM = N / E, NTF = 8, NTHREADS = NTF * TEAM;
+    // team buffers [NTF][N] | curr of the three fields [3][N] | 64 doubles of diagnostic sums
+    static constexpr size_t SMEM = (size_t)(NTF + 3) * N * sizeof(cplx<real>) + 64 * sizeof(double);
+    static_assert(N >= 32 && N <= 256, "small grids (whole warps of threads)");
+};
+
+template <typename real, int N, int E>
+__global__ void __launch_bounds__(ColFP<real, N, E>::NTHREADS) colfp_kernel(const __grid_constant__ StageArgs<real> a) {
+    using K = ColFP<real, N, E>;
+    constexpr int TEAM = K::TEAM, NTF = K::NTF, NT = K::NTHREADS, H = N / 2;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cplx<real>* sm = reinterpret_cast<cplx<real>*>(smem_raw);
+    const int tid = threadIdx.x;
+    if ((int)blockIdx.x >= H) {   // edge CTAs: field blockIdx.x - H, NTF teams share its transforms
+        col_edge<real, N, NTF, E, true>(a, (int)blockIdx.x - H, 0, tid / NTF, tid % NTF, sm, sm + (size_t)N * NTF);
+        return;
+    }
+    const int g = tid / TEAM, t = tid % TEAM;   // team g (G_g forward, Y_g inverse), transform index t
+    const int i = (int)blockIdx.x;              // the kx-column
+    const bool edge_col = (i == 0);             // kx = 0 belongs to the edge CTAs
+    cplx<real>* cur = sm + (size_t)NTF * N;     // curr of field f at cur[f * N + j]
+    double* red = reinterpret_cast<double*>(sm + (size_t)(NTF + 3) * N);
+    XchgCols<real> x{sm + (size_t)g * N, 0, 1};
+    TeamFFT<real, N, E> fft;
+    fft.template init<N>(t, a.tw_y);
+    const real kx = a.dkx * (real)i;
+    const real sc = (real)1 / ((real)N * (real)N);
+    cplx<real> v[E];
+
+    // forward: team g < NG transforms column i of G_g and leaves ky^pow F_y(G_g)
+    // in its buffer (pow 0, 1, 2 for G0-G2 of w; 0, 1 for G3-G4 of r1 and G5-G6 of r2)
+    if (a.mode != MODE_PROLOGUE) {
+        const bool act = g < NG;
+        const cplx<real>* Gc = a.G + (size_t)(act ? g : 0) * N * H + i;
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = act ? Gc[(size_t)(t + TEAM * e) * H] : mk<real>(0, 0);
+        fft.template run<false>(t, v, x);
+        const int pw = (g == 0 || g == 3 || g == 5) ? 0 : (g == 2 ? 2 : 1);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const real ky = ky_of<real>(t + TEAM * e, N, a.dky);
+            const real m = pw == 0 ? (real)1 : (pw == 1 ? ky : ky * ky);
+            x.write(t + TEAM * e, cscale(v[e], m));
+        }
+        __syncthreads();
+    }
+
+    // stage update of the three fields at every ky of the column
+    const bool need_old = a.mode == MODE_PROLOGUE || (a.mode == MODE_STAGE &&
+                          (a.integrator == INT_IFE || (a.integrator == INT_IFRK4 && a.stage <= 3) ||
+                           (a.integrator == INT_IFRK2 && a.stage == 1)));
+    const bool need_acc = a.mode == MODE_STAGE && ((a.integrator == INT_IFRK4 && a.stage >= 2) ||
+                                                   (a.integrator == INT_IFRK2 && a.stage == 2));
+    double zsum = 0, esum = 0;
+    bool bad = false;
+    for (int it = tid; it < 3 * N; it += NT) {
+        const int f = it / N, j = it % N;
+        const size_t li = tidx(N, i, j);
+        cplx<real> nl = mk<real>(0, 0);
+        if (a.mode != MODE_PROLOGUE) {
+            const int g0 = f == 0 ? 0 : (f == 1 ? 3 : 5), ng = f == 0 ? 3 : 2;
+            for (int gg = 0; gg < ng; ++gg) nl = cadd(nl, sm[(size_t)(g0 + gg) * N + j]);
+        }
+        if (a.mode == MODE_NONL) {
+            if (!edge_col) pick3(a.nl_m, f)[li] = nl;
+            continue;
+        }
+        cplx<real> c;
+        if (a.mode == MODE_PROLOGUE) {
+            c = pick3(a.old_m, f)[li];
+        } else {
+            const int cls = f == 0 ? 0 : 2;
+            const real* e0 = a.inst_e0 ? a.inst_e0 : a.e0;
+            const real exf = a.ex[cls * (H + 1) + i] * e0[cls];
+            const real exh = a.ex[(cls + 1) * (H + 1) + i] * e0[cls + 1];
+            const real Ef = exf * a.ey[cls * N + j], Eh = exh * a.ey[(cls + 1) * N + j];
+            const cplx<real> o = need_old ? pick3(a.old_m, f)[li] : mk<real>(0, 0);
+            const cplx<real> ac = need_acc ? pick3(a.acc_m, f)[li] : mk<real>(0, 0);
+            const StageUpdate<real> u = stage_update(a, nl, o, ac, Ef, Eh, mask_keep(a, f, i, j));
+            if (!edge_col) {
+                if (u.write_acc) pick3(a.acc_m, f)[li] = u.acc;
+                if (u.write_old) {
+                    pick3(a.old_m, f)[li] = u.acc;
+                    bad |= !(isfinite(u.acc.x) && isfinite(u.acc.y));
+                    if (f == 0 && a.diag) {
+                        const real ky = ky_of<real>(j, N, a.dky);
+                        const double k2 = (double)kx * kx + (double)ky * ky;
+                        const double m2 = (double)u.acc.x * u.acc.x + (double)u.acc.y * u.acc.y;
+                        zsum += 2.0 * m2;
+                        if (k2 > 0) esum += 2.0 * m2 / k2;
+                    }
+                }
+            }
+            c = u.curr;
+        }
+        cur[(size_t)f * N + j] = c;
+    }
+    if (a.mode == MODE_STAGE && a.last_stage) {
+        if (a.flags && __any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(a.flags, FLAG_NONFINITE);
+        if (a.diag) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                zsum += __shfl_xor_sync(0xffffffffu, zsum, o);
+                esum += __shfl_xor_sync(0xffffffffu, esum, o);
+            }
+            if ((tid & 31) == 0) { red[2 * (tid >> 5)] = zsum; red[2 * (tid >> 5) + 1] = esum; }
+        }
+    }
+    __syncthreads();
+    if (a.mode == MODE_STAGE && a.last_stage && a.diag && tid == 0) {
+        double z = 0, en = 0;
+        for (int k = 0; k < NT / 32; ++k) { z += red[2 * k]; en += red[2 * k + 1]; }
+        atomicAdd(&a.diag[0], z);
+        atomicAdd(&a.diag[1], en);
+    }
+    if (a.mode == MODE_NONL || !a.do_inverse) return;
+
+    // inverse: team q = g transforms the multiplied curr of its field into Y_q
+    const int q = g, fq = (q == 1 || q == 6) ? 1 : ((q == 2 || q == 7) ? 2 : 0);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int j = t + TEAM * e;
+        const real ky = ky_of<real>(j, N, a.dky);
+        v[e] = y_mult<real>(q, cur[(size_t)fq * N + j], ky, kx * kx + ky * ky, sc);
+    }
+    fft.template run<true>(t, v, x);
+    cplx<real>* Y = a.Y + (size_t)q * N * H + i;
+#pragma unroll
+    for (int e = 0; e < E; ++e) Y[(size_t)(t + TEAM * e) * H] = v[e];
+}
+
 template <typename real, int N, int E, int MINB, int MODE = 0, bool SQ = true>
 __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_constant__ StageArgs<real> a) {
     using K = ColKernel<real, N, E, MODE, SQ>;

@@ -39,6 +39,9 @@ qaf_status Launch<real, N>::setup() {
         QAF_CUDA(cudaFuncSetAttribute(row_kernel<real, N, C::ER, C::ROWS, C::MINB, 0, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::ROW_SMEM));
         QAF_CUDA(cudaFuncSetAttribute(col_ifft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
+        if constexpr (C::COL_FP)
+            QAF_CUDA(cudaFuncSetAttribute(colfp_kernel<real, N, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)ColFP<real, N, C::EC>::SMEM));
         QAF_CUDA(cudaFuncSetAttribute(col_fft_kernel<real, N, C::W, C::EC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::COLT_SMEM));
         int dev = 0, sms = 0, per_sm = 0;
         QAF_CUDA(cudaGetDevice(&dev));
@@ -71,6 +74,15 @@ void Launch<real, N>::col(const StageArgs<real>& a0, cudaStream_t st) {
                 v->launch(a, slots, st);
                 return;
             }
+        }
+    }
+    // a single small square grid: the field-parallel column pass (a test
+    // hook's launch, which withholds one of the persistent kernel's copies,
+    // keeps the persistent kernel)
+    if constexpr (C::COL_FP) {
+        if (a.ninst == 1 && a.nx == N && a.drop_slab == 0) {
+            colfp_kernel<real, N, C::EC><<<N / 2 + 3, ColFP<real, N, C::EC>::NTHREADS, ColFP<real, N, C::EC>::SMEM, st>>>(a);
+            return;
         }
     }
     const long items = (long)(2 * (a.nx / 2 / TW) + 3) * a.ninst;
