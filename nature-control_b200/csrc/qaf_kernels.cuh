@@ -93,7 +93,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsign
 // and the integrating factors' ky table in shared memory (for launches of
 // one CTA per SM, which leave the room); MODE 3 / 4: MODE 2 with a copy ring
 // of 4 / 5 slabs. +16: the double-buffered exchange swizzled (XOR of an
-// index's low two bits with bits of idx / E).
+// index's low two bits with bits of idx / E). +64: the item code compiled
+// once (ONE_BODY).
 //
 // N is the column length ny (the y-transforms' length); the number of
 // kx-columns H = nx / 2, and with it the tiles and work items, is a launch
@@ -107,6 +108,9 @@ struct ColKernel {
     static constexpr bool DB = BASE >= 2;            // double-buffered exchange, ky factors in shared memory
     static constexpr int NBUF = BASE == 3 ? 4 : (BASE >= 4 ? 5 : 3);   // slab buffers in the copy ring
     static constexpr bool SWZ = DB && (MODE & 16) && E % 4 == 0;
+    // +64 (with MODE 1 or above): the item code once — the two fields of an
+    // item in a loop and both item kinds through one call
+    static constexpr bool ONE_BODY = SB && (MODE & 64);
     // elements whose IF factors are fetched ahead of the stage-update stores;
     // at 1024^2 the extra live registers cost more in spills than they save
     static constexpr int PF = N >= 1024 ? 1 : (E < 4 ? E : 4);
@@ -418,7 +422,16 @@ struct ColKernel {
         nseq = per_a + (fb >= 0 ? per_field(fb) : 0);
         next = 0;
         issue_upto(NBUF);
-        if constexpr (INLINE_ITEM) {
+        if constexpr (ONE_BODY) {
+            // one copy of the field code for both fields (and, through the
+            // kernel's single call, both item kinds): less code to fetch
+#pragma unroll 1
+            for (int k = 0; k < 2; ++k) {
+                const int f = k == 0 ? fa : fb;
+                if (f < 0) break;
+                field_body(f, k == 0 ? 0 : per_a);
+            }
+        } else if constexpr (INLINE_ITEM) {
             field_body(fa, 0);
             if (fb >= 0) field_body(fb, per_a);
         } else {
@@ -859,7 +872,10 @@ __global__ void __launch_bounds__(TW * (N / E), MINB) col_kernel(const __grid_co
         if (q >= total) break;
         k.q_cur = q;
         const int local = q / a.ninst, inst = q % a.ninst;
-        if (local < tiles) {
+        if (K::ONE_BODY && local < 2 * tiles) {
+            const bool rp = local < tiles;   // r1 + r2 of tile `local`, else w of tile local - tiles
+            k.item_body(rp ? 1 : 0, rp ? 2 : -1, rp ? local : local - tiles, inst);
+        } else if (local < tiles) {
             if constexpr (K::INLINE_ITEM) k.item_body(1, 2, local, inst);
             else k.item(1, 2, local, inst);
         } else if (local < 2 * tiles) {
