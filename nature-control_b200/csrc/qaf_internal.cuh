@@ -131,16 +131,20 @@ struct Cfg {
     // The small FP32 grids take the shapes that timed fastest on the B200
     // when every shape was timed on one box (single grid and an 85-instance
     // batch each): 64^2 four values per column thread (26-28% faster than
-    // eight), 256^2 batches six column CTAs per SM with register twiddle
-    // bases (2%), 128^2 and 256^2 single grids two rows per row CTA (5-9%).
+    // eight), 128^2 and 256^2 batches six column CTAs per SM, 128^2 and
+    // 256^2 single grids two rows per row CTA (5-9%).
     static constexpr bool WIDE1024 = F32 && N == 1024;
     static constexpr int ECS = WIDE1024 || (F32 && N == 64) ? 4 : EC;
-    // (+64 with the shared table: the item code compiled once, ColKernel::ONE_BODY)
-    static constexpr int COL_MODE = WIDE1024 ? QAF_COL1024_MODE : (((F32 && N == 768) || (!F32 && N >= 512)) ? 65 : 0);
+    // (+64 with the shared table: the item code compiled once, ColKernel::ONE_BODY;
+    // measured per step on one box, batches of 85: 64^2 214 -> 177 us,
+    // 128^2 645 -> 592 us, 256^2 2002 -> 1548 us with six CTAs per SM; a
+    // single 64^2 grid 120 -> 111 us)
+    static constexpr int COL_MODE = WIDE1024 ? QAF_COL1024_MODE
+                                             : (((F32 && (N == 768 || N == 64)) || (!F32 && N >= 512)) ? 65 : 0);
     // batches of instances
-    static constexpr int COL_MODE_B = WIDE1024 ? QAF_COL1024_MODE : ((F32 && (N == 64 || N == 256)) ? 0 : 65);
+    static constexpr int COL_MODE_B = WIDE1024 ? QAF_COL1024_MODE : 65;
     static constexpr int MINBC = WIDE1024 ? 1 : MINB;
-    static constexpr int MINBC_B = (F32 && N == 256) ? 6 : MINBC;
+    static constexpr int MINBC_B = (F32 && (N == 128 || N == 256)) ? 6 : MINBC;
     // batches launch their own kernel where its shape differs from the single grids'
     static constexpr bool SEP_B = COL_MODE_B != COL_MODE || MINBC_B != MINBC;
     // single square grids of 32^2, 128^2 and 256^2: the field-parallel column
