@@ -71,8 +71,30 @@ double check() {
 #define CASE(real, L, E, INV, TOL) do { double e = check<real, L, E, INV>(); \
     std::printf("%-6s L=%-5d E=%-3d inv=%d rel=%.3e\n", #real, L, E, (int)INV, e); if (!(e < TOL)) bad++; } while (0)
 
+// The row kernels' R2C unpack pairs Z[k] (k = t + TEAM e, e < E/2) with
+// Z[L - k]; where a team lies within one warp it reads the partner by warp
+// shuffle from lane (TEAM - t) % TEAM, register E - 1 - e (t > 0), or from its
+// own register (E - e) % E (t = 0), and Z[L/2] from its own register E/2.
+// Checks that map against the distribution "thread t holds t + TEAM e".
+bool partner_map_ok(int L, int E) {
+    const int TEAM = L / E;
+    for (int t = 0; t < TEAM; ++t)
+        for (int e = 0; e < E / 2; ++e) {
+            const int k = t + TEAM * e;
+            if (k == 0) continue;
+            const int m = (L - k) % L;
+            const int lane = (TEAM - t) % TEAM, reg = t == 0 ? (E - e) % E : E - 1 - e;
+            if (m % TEAM != lane || m / TEAM != reg) return false;
+        }
+    return (L / 2) % TEAM == 0 && (L / 2) / TEAM == E / 2;
+}
+
 int main() {
     int bad = 0;
+    // the shuffle unpack's lanes and registers for the row shapes that use it (team <= 32 threads)
+    const int pm[][2] = {{32, 8}, {48, 12}, {64, 8}, {96, 12}, {128, 8}, {192, 12}, {256, 8}, {64, 4}, {128, 4}};
+    for (const auto& c : pm)
+        if (!partner_map_ok(c[0], c[1])) { std::printf("R2C partner map wrong at L=%d E=%d\n", c[0], c[1]); bad++; }
     // the exchange swizzle permutes every buffer length the kernels use (8 .. 8192 elements)
     for (int len = 8; len <= 8192; len = (len % 3 == 0) ? len * 4 / 3 : (len >= 16 ? len * 3 / 2 : len * 2)) {
         std::vector<int> seen(len, 0);
